@@ -1,0 +1,132 @@
+"""NumPy FP64 restatement of the reference's MALA/DEER formulas (TEST INFRASTRUCTURE ONLY).
+
+An independent second restatement used to cross-check the C oracle on small
+cases.  Each function cites the reference file:line it follows.  Arrays use the
+(D, T) convention of oracle.py.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _softplus(z):
+    return np.maximum(z, 0.0) + np.log1p(np.exp(-np.abs(z)))
+
+
+class NPTarget:
+    """kind in {'diag', 'dense', 'logistic'} with logp/grad/hvp closures."""
+
+    def __init__(self, kind, prec=None, mean=None, X=None, y=None, prior_prec=1.0):
+        self.kind = kind
+        if kind == "diag":
+            lam = np.asarray(prec, float)
+            m = np.zeros_like(lam) if mean is None else np.asarray(mean, float)
+            self.D = lam.size
+            self.logp = lambda x: -0.5 * np.sum(lam * (x - m) ** 2)
+            self.grad = lambda x: -lam * (x - m)
+            self.hvp = lambda x, v: -lam * v
+        elif kind == "dense":
+            P = np.asarray(prec, float)
+            m = np.zeros(P.shape[0]) if mean is None else np.asarray(mean, float)
+            self.D = P.shape[0]
+            self.logp = lambda x: -0.5 * (x - m) @ P @ (x - m)
+            self.grad = lambda x: -P @ (x - m)
+            self.hvp = lambda x, v: -P @ v
+        else:
+            Xm = np.asarray(X, float)
+            yv = np.asarray(y, float)
+            tau = float(prior_prec)
+            self.D = Xm.shape[1]
+            # bayes_logreg.jl:37-58, 76-83
+            self.logp = lambda b: float(np.sum(yv * -_softplus(-(Xm @ b)) +
+                                               (1 - yv) * -_softplus(Xm @ b))
+                                        - 0.5 * tau * b @ b)
+            self.grad = lambda b: Xm.T @ (yv - 1 / (1 + np.exp(-(Xm @ b)))) - tau * b
+
+            def hvp(b, v):
+                p = 1 / (1 + np.exp(-(Xm @ b)))
+                return -Xm.T @ (p * (1 - p) * (Xm @ v)) - tau * v
+
+            self.hvp = hvp
+
+
+def logq(tg, y, x, gx, eps):
+    """logq_mala! (MALA.jl:172-193), identity mass matrix."""
+    r = y - (x + eps * gx)
+    return -0.5 * (r @ r) / (2 * eps) - (x.size / 2) * np.log(4 * np.pi * eps)
+
+
+def mala_step(tg, eps, x, xi, u):
+    """mala_step_with_logalpha! (MALA.jl:377-411)."""
+    gx = tg.grad(x)
+    y = x + eps * gx + np.sqrt(2 * eps) * xi
+    gy = tg.grad(y)
+    la = (tg.logp(y) + logq(tg, x, y, gy, eps)) - (tg.logp(x) + logq(tg, y, x, gx, eps))
+    acc = np.log(u) < la
+    return (y.copy() if acc else x.copy()), bool(acc), la
+
+
+def mala_sequential(tg, eps, x0, Xi, u):
+    """run_mala_sequential_taped (MALA.jl:322-346); S[:, t] = x_{t+1}."""
+    D, T = Xi.shape
+    S = np.empty((D, T))
+    acc = np.zeros(T, bool)
+    x = np.asarray(x0, float)
+    for t in range(T):
+        x, acc[t], _ = mala_step(tg, eps, x, Xi[:, t].astype(float), float(u[t]))
+        S[:, t] = x
+    return S, acc
+
+
+def fwd_and_jvp(tg, eps, x, xi, u, v):
+    """mala_step_taped_and_jvp! (MALA.jl:732-797)."""
+    gx = tg.grad(x)
+    y = x + eps * gx + np.sqrt(2 * eps) * xi
+    gy = tg.grad(y)
+    la = (tg.logp(y) + logq(tg, x, y, gy, eps)) - (tg.logp(x) + logq(tg, y, x, gx, eps))
+    g = 1 / (1 + np.exp(-(la - np.log(u))))
+    a = 1.0 if np.log(u) < la else 0.0
+    w = v + eps * tg.hvp(x, v)
+    r = x - y - eps * gy
+    dr = v - w - eps * tg.hvp(y, w)
+    dla = np.sum(gy * w - gx * v - (1 / (2 * eps)) * r * dr)
+    dg = g * (1 - g) * dla
+    return (y if a else x), a * w + (y - x) * dg + (1 - a) * v
+
+
+def scan_seq(A, B, s0):
+    """solve_affine_seq! (DEERScan.jl:51-68)."""
+    D, T = A.shape
+    S = np.empty((D, T))
+    s = np.asarray(s0, float)
+    for t in range(T):
+        s = A[:, t] * s + B[:, t]
+        S[:, t] = s
+    return S
+
+
+def deer_update(tg, eps, s0, S_in, Xi, u, Zs, jacobian="stoch_diag", damping=0.5):
+    """deer_update! (DEER.jl:375-475) with explicit probes Zs (list of (D,T))."""
+    D, T = S_in.shape
+    Xbar = np.concatenate([np.asarray(s0, float)[:, None], S_in[:, :T - 1]], axis=1)
+    A = np.zeros((D, T))
+    B = np.zeros((D, T))
+    for t in range(T):
+        xb = Xbar[:, t]
+        xi = Xi[:, t].astype(float)
+        if jacobian == "stoch_diag":
+            acc = np.zeros(D)
+            for Z in Zs:
+                ft, jv = fwd_and_jvp(tg, eps, xb, xi, float(u[t]), Z[:, t])
+                acc += Z[:, t] * jv
+            jt = acc / len(Zs)
+        else:
+            ft, _, _ = mala_step(tg, eps, xb, xi, float(u[t]))
+            jt = np.array([fwd_and_jvp(tg, eps, xb, xi, float(u[t]), e)[1][i]
+                           for i, e in enumerate(np.eye(D))])
+        A[:, t] = jt
+        B[:, t] = ft - jt * xb
+    S = scan_seq(A, B, s0)
+    if damping != 1.0:
+        S = (1 - damping) * S_in + damping * S
+    return S, A, B
