@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""DEER samples/sec on one B200 (or N replicas, one per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one DEER block solved to convergence, tape generation
+and per-sample logp included): the anisotropic diagonal Gaussian, D = 100,
+precisions log-uniform in [1e-2, 1e2] (seed 1), eps = 0.05, T = 16384,
+jacobian = :diag, FP32 state, x0 ~ N(0, I), sampler defaults otherwise.
+The path does not shard (one chain), so N GPUs run N independent replicas
+(different tape seeds): weak scaling, no data-path collective.
+
+Printed JSON: value = device-timed samples/s with inputs resident in HBM (L2
+flushed between steps), e2e = the same through pmcmc.sample() with host
+buffers, plain_gpu = the unfused reference-structured GPU path, roofline of
+the sweep kernel, cpu_baseline = the FP64 CPU restatement of the reference
+algorithm on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parallelmcmc.jl_b200"))
+
+METRIC = "DEER samples/sec, batched+mixed vs plain GPU DEER, at trace err ≤1e-5 vs FP64"
+WORKLOAD = "diag_gauss_D100_T16384_diag_f32"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+L2_FLUSH_BYTES = 512 << 20
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, parts[2:]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_block(model, sampler, x0, seed, block, nthreads):
+    """The FP64 CPU restatement of the reference algorithm (per-t :diag with D JVPs
+    per column, DEER.jl:420-468; Hillis-Steele scan, DEERScan.jl:102-173) on one block."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    tg = model.target
+    otg = O.Target.diag_gauss(tg["prec"], tg["mean"])
+    Xi, u = O.tape(seed, block, model.dim, sampler.T)
+    t0 = time.perf_counter()
+    S, info = O.deer_solve(otg, sampler.epsilon, np.asarray(x0, np.float64), Xi, u, seed, block,
+                           jacobian=sampler.jacobian, damping=sampler.damping,
+                           tol_abs=sampler.tol_abs, tol_rel=sampler.tol_rel,
+                           maxiter=sampler.maxiter, probes=sampler.probes, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return S, info, dt
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    from pmcmc import configs
+    model, sampler, x0, meta = configs.aniso_diag_d100()
+    nthreads = os.cpu_count() or 1
+    for w in range(args.warmup):
+        cpu_reference_block(model, sampler, x0, meta["seed"], w, nthreads)
+    times, iters = [], []
+    for k in range(args.steps):
+        _, info, dt = cpu_reference_block(model, sampler, x0, meta["seed"], args.warmup + k,
+                                          nthreads)
+        times.append(dt)
+        iters.append(info["iters"])
+    total = sum(times)
+    value = args.steps * sampler.T / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, see config)",
+        "config": {"workload": WORKLOAD, "D": 100, "T": sampler.T, "eps": 0.05,
+                   "jacobian": "diag", "newton_iters_mean": statistics.mean(iters)},
+        "cpu_baseline": {"value": value, "unit": "samples/s", "cores": nthreads, "kind": "port",
+                         "sample": "full blocks: FP64 C restatement of the reference CPU DEER "
+                                   "(per-t :diag with D JVPs per column, doubling scan), OpenMP"},
+        "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "Julia is not installed; the reference arm is the oracle port of its algorithm",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import pmcmc
+    from pmcmc import _lib as L
+    from pmcmc import configs
+
+    world, rank, local = dist_setup()
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    h = pmcmc.Handle(local, stream=stream.cuda_stream)
+    lib = L.load()
+
+    model, sampler, x0, meta = configs.aniso_diag_d100()
+    D, T = model.dim, sampler.T
+    seed = meta["seed"] + 7919 * rank  # replicas: each rank its own tape stream
+    tgt = model.device_target(h)
+    x0_dev = torch.from_numpy(np.asarray(x0)).to(dev)
+    S_dev = torch.empty((T, D), dtype=torch.float32, device=dev)
+    lp_dev = torch.empty((T,), dtype=torch.float32, device=dev)
+    acc_dev = torch.empty((T,), dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def solve_dev(smp, block):
+        info = L.Info()
+        p = smp.params()
+        rc = lib.pmcmc_deer_solve(h.ptr, tgt, C.byref(p), x0_dev.data_ptr(), seed, block,
+                                  S_dev.data_ptr(), lp_dev.data_ptr(), acc_dev.data_ptr(),
+                                  L.MEM_DEVICE, C.byref(info))
+        L.check(rc, h.ptr, "deer_solve")
+        return info
+
+    def timed(smp, nsteps, block0):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(nsteps)]
+        infos = []
+        for k in range(nsteps):
+            flush.zero_()  # L2 flush (512 MB > 126 MB L2), outside the timed events
+            ev[k][0].record(stream)
+            infos.append(solve_dev(smp, block0 + k))
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in ev], infos
+
+    # ---- warm-up and timed region (device-resident inputs/outputs)
+    timed(sampler, args.warmup, 0)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ms, infos = timed(sampler, args.steps, 1000)
+    torch.cuda.synchronize(dev)
+    total_ms = sum(ms)
+    if pg:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * T / (total_ms / 1e3)
+    iters = [i.iters for i in infos]
+    launches = sum(2 + i.iters for i in infos)  # init + sweeps + finalize per block
+
+    # ---- parity of the timed workload: first timed block vs the FP64 sequential oracle
+    parity = {}
+    if rank == 0:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            solve_dev(sampler, 1000)
+            S = S_dev.cpu().numpy().T.astype(np.float64)
+            acc = acc_dev.cpu().numpy().astype(bool)
+            Xi, u = O.tape(seed, 1000, D, T)
+            otg = O.Target.diag_gauss(model.target["prec"])
+            S_seq, acc_seq, _ = O.mala_sequential(otg, sampler.epsilon,
+                                                  np.asarray(x0, np.float64), Xi, u)
+            err = float(np.max(np.linalg.norm(S - S_seq, axis=0) /
+                               np.maximum(np.linalg.norm(S_seq, axis=0), 1e-30)))
+            parity = {"trace_err_vs_fp64": err, "accept_identical": bool(np.array_equal(acc, acc_seq)),
+                      "accept_rate": float(acc.mean())}
+        except Exception as e:  # parity is reported, never fatal for the timing
+            parity = {"error": repr(e)}
+
+    # ---- plain GPU DEER (unfused, reference-structured) on the same workload
+    plain = pmcmc.ParallelMALASampler(sampler.epsilon, T=T, jacobian=sampler.jacobian,
+                                      dtype=np.float32, exec="plain")
+    timed(plain, 1, 0)
+    pms, pinfos = timed(plain, max(3, args.steps // 4), 2000)
+    plain_value = len(pms) * T / (sum(pms) / 1e3)
+
+    # ---- roofline of the dominant kernel (the fused sweep), CUDA events per launch
+    h.set_profiling(True)
+    for k in range(max(3, args.steps // 2)):
+        flush.zero_()
+        solve_dev(sampler, 3000 + k)
+    torch.cuda.synchronize(dev)
+    prof = h.profile(reset=True)
+    h.set_profiling(False)
+    sweep_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
+    alg_bytes = 12 * D * T + 8 * T  # per sweep launch (S read, Xi read, S write, u read, logp write)
+    min_bytes = 8 * D * T + 4 * T  # what this kernel must move (tape regenerated in registers)
+    hbm, src = peaks()
+    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+
+    # ---- end to end through the public API with host buffers
+    x0_host = np.asarray(x0, np.float32)
+    pmcmc.sample(model, sampler, T, seed=seed, initial_params=x0_host, handle=h)
+    e2e_t = []
+    for k in range(max(3, args.steps // 2)):
+        t0 = time.perf_counter()
+        pmcmc.sample(model, sampler, T, seed=seed + 1 + k, initial_params=x0_host, handle=h)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_local = len(e2e_t) * T / sum(e2e_t)
+    e2e_val = e2e_local
+    if pg:
+        t = torch.tensor([sum(e2e_t)], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_val = world * len(e2e_t) * T / float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        _, cinfo, cdt = cpu_reference_block(model, sampler, x0, seed, 0, nthreads)
+        cpu = {"value": T / cdt, "unit": "samples/s", "cores": nthreads, "kind": "port",
+               "sample": f"one full block (T={T}): FP64 C restatement of the reference CPU DEER "
+                         f"(per-t :diag, D JVPs per column, doubling scan), "
+                         f"{cinfo['iters']} Newton iterations, OpenMP"}
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded NumPy PCG64 + counter-based Philox tape)",
+            "config": {"workload": WORKLOAD, "D": D, "T": T, "eps": 0.05, "jacobian": "diag",
+                       "state": "f32", "logalpha": "f64", "l2": "flushed (512 MB write) "
+                       "between timed steps", "parallelism": f"replicas x{world}",
+                       "newton_iters_mean": statistics.mean(iters)},
+            "e2e": {"value": e2e_val, "unit": "samples/s", "h2d_bytes_per_step": 4 * D,
+                    "d2h_bytes_per_step": 4 * D * T + 4 * T + T},
+            "plain_gpu": {"value": plain_value, "unit": "samples/s",
+                          "newton_iters_mean": statistics.mean(i.iters for i in pinfos),
+                          "speedup_fused_over_plain": value / world / plain_value},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "kernel": "deer_sweep_kernel", "avg_launch_ms": sweep_ms,
+                         "alg_bytes_per_launch": alg_bytes,
+                         "kernel_min_bytes_per_launch": min_bytes,
+                         "launches_profiled": prof["sweep_launches"]},
+            "cpu_baseline": cpu,
+            "parity": parity,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+/*
+ * pmcmc_deer.h -- C ABI of libpmcmc_deer.so, the B200 (sm_100a) DEER hot path of
+ * ParallelMCMC.jl.
+ *
+ * The library replaces everything below `_deer_solve_new_tape`
+ * (src/interface.jl:475-515): tape generation, the batched MALA forward +
+ * Jacobian estimate (src/MALA/MALA.jl:556-628), the Newton loop of
+ * `DEER.solve` (src/DEER/DEER.jl:506-595) with `deer_update!`
+ * (src/DEER/DEER.jl:375-475) and the diagonal affine scan
+ * (src/DEER/DEERScan.jl:102-173).  Callers keep `mcmcsample`, `step` and the
+ * FlexiChains bundling; a Julia `ccall` (or Python ctypes) binding calls these
+ * functions with plain pointers.
+ *
+ * Conventions
+ *  - Trajectories are D x T column-major, column t (state t) contiguous, like
+ *    the reference's Julia matrices (src/DEER/DEER.jl:451-452).
+ *  - Every data pointer is either host or device memory; `mem` flags
+ *    (PMCMC_MEM_*) say which.  Device pointers must belong to the handle's
+ *    device.  Host buffers need not be pinned.
+ *  - Element type of state buffers follows `pmcmc_deer_params.dtype`
+ *    (PMCMC_F32 -> float, PMCMC_F64 -> double), as the reference's working
+ *    precision follows typeof(epsilon) (src/interface.jl:276-277).
+ *  - Return value: PMCMC_OK or an error code; pmcmc_last_error() gives the
+ *    message.  ArgumentError / DimensionMismatch of the reference map to
+ *    PMCMC_ERR_ARGUMENT / PMCMC_ERR_DIMENSION.  Non-convergence is not an
+ *    error (the reference accepts it silently, src/interface.jl:501-513); it
+ *    is reported in pmcmc_info.converged.
+ *  - Threading: one handle per host thread / stream.  Calls on distinct
+ *    handles are independent (AbstractMCMC MCMCThreads, test-DEER-Interface.jl:300-318).
+ */
+#ifndef PMCMC_DEER_H
+#define PMCMC_DEER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMCMC_ABI_VERSION 1
+
+typedef enum {
+  PMCMC_OK = 0,
+  PMCMC_ERR_ARGUMENT = 1,    /* reference: ArgumentError */
+  PMCMC_ERR_DIMENSION = 2,   /* reference: DimensionMismatch */
+  PMCMC_ERR_CUDA = 3,        /* CUDA runtime error */
+  PMCMC_ERR_NONFINITE = 4,   /* NaN/Inf reached the trajectory */
+  PMCMC_ERR_TIMEOUT = 5,     /* a bounded device wait gave up (never hangs) */
+  PMCMC_ERR_UNSUPPORTED = 6, /* valid request this build does not implement */
+  PMCMC_ERR_NOMEM = 7
+} pmcmc_status;
+
+typedef enum { PMCMC_JAC_STOCH_DIAG = 0, PMCMC_JAC_DIAG = 1, PMCMC_JAC_FULL = 2 } pmcmc_jacobian;
+typedef enum { PMCMC_F32 = 0, PMCMC_F64 = 1 } pmcmc_dtype;
+typedef enum { PMCMC_MEM_HOST = 0, PMCMC_MEM_DEVICE = 1 } pmcmc_mem;
+
+/* Execution strategy of a solve.
+ * PMCMC_EXEC_FUSED: one fused kernel per Newton sweep, the Newton loop in a
+ *   CUDA graph with a device-side convergence test (the product path).
+ * PMCMC_EXEC_PLAIN: the reference's structure on the GPU -- separate
+ *   broadcast-style kernels, Hillis-Steele doubling scan, host-synchronised
+ *   convergence check every iteration, FP32 SIMT only (the "plain GPU DEER"
+ *   baseline of the north-star metric). */
+typedef enum { PMCMC_EXEC_FUSED = 0, PMCMC_EXEC_PLAIN = 1 } pmcmc_exec;
+
+typedef struct pmcmc_handle pmcmc_handle;
+typedef struct pmcmc_target pmcmc_target;
+
+/* ParallelMALASampler fields (src/interface.jl:248-290) plus the north-star
+ * additions (:full, window) and execution controls. */
+typedef struct {
+  double epsilon;   /* step size, > 0 */
+  int64_t T;        /* trajectory length per block (reference default 64) */
+  int32_t maxiter;  /* Newton iterations (default 200) */
+  double tol_abs;   /* default 1e-6 */
+  double tol_rel;   /* default 1e-5 */
+  int32_t jacobian; /* pmcmc_jacobian (default STOCH_DIAG) */
+  double damping;   /* in (0, 1] (default 0.5) */
+  int32_t probes;   /* Hutchinson probes >= 1 (default 1) */
+  int64_t window;   /* sliding window width; 0 = whole block */
+  int32_t dtype;    /* pmcmc_dtype of state buffers */
+  int32_t exec;     /* pmcmc_exec */
+} pmcmc_deer_params;
+
+/* DEER.solve info (src/DEER/DEER.jl:585-594) plus parity diagnostics. */
+typedef struct {
+  int32_t iters;       /* Newton sweeps run */
+  int32_t converged;   /* metric <= 1 reached */
+  double metric;       /* max|dS| / (tol_abs + tol_rel max|S|), FP64 */
+  int64_t n_accept;    /* accepted proposals on the returned trajectory */
+  double min_margin;   /* min_t |logalpha_t - log u_t| (FP64) */
+  double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory */
+  int32_t status;      /* pmcmc_status of the device work */
+  int32_t reserved;
+} pmcmc_info;
+
+/* ---- handle ------------------------------------------------------------ */
+/* Replaces DEERWorkspace (src/DEER/DEER.jl:47-90): owns all device workspace,
+ * reused across blocks and solves.  `stream` may be NULL (handle creates one). */
+int pmcmc_create(int device, void* stream, pmcmc_handle** out);
+int pmcmc_destroy(pmcmc_handle* h);
+const char* pmcmc_last_error(const pmcmc_handle* h);
+int pmcmc_abi_version(void);
+
+/* ---- targets -------------------------------------------------------------
+ * Replace the user closures of DensityModel (src/interface.jl:36-70) with
+ * built-in device targets.  Parameters are copied to the device at creation.
+ * Diagonal Gaussian: logp = -1/2 sum_i prec_i (x_i - mean_i)^2
+ *   (test-DEER-Interface.jl:13-16, test-GPU-MALA.jl:34-44).
+ * Dense Gaussian: logp = -1/2 (x-mean)' P (x-mean), P symmetric D x D.
+ * Logistic regression (bayes_logreg.jl:30-86, 91-206): X is N x D
+ *   column-major (Julia), y in {0,1}, prior N(0, prior_prec^-1 I).
+ * `mean` may be NULL (zero).  All pointers are host memory. */
+int pmcmc_target_diag_gauss(pmcmc_handle* h, int64_t D, const double* mean, const double* prec,
+                            pmcmc_target** out);
+int pmcmc_target_dense_gauss(pmcmc_handle* h, int64_t D, const double* mean,
+                             const double* prec, pmcmc_target** out);
+int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X,
+                          const double* y, double prior_prec, pmcmc_target** out);
+int pmcmc_target_destroy(pmcmc_target* t);
+
+/* ---- tape ------------------------------------------------------------------
+ * Counter-based replacement of _make_mala_tape_block (src/interface.jl:334-358):
+ * writes Xi (D x T, float) and u (T, float) for (seed, block). */
+int pmcmc_tape(pmcmc_handle* h, int64_t D, int64_t T, uint64_t seed, uint64_t block, float* Xi,
+               float* u, int32_t mem);
+
+/* ---- one DEER block ---------------------------------------------------------
+ * Replaces _deer_solve_new_tape + DEER.solve + _trajectory_logps
+ * (src/interface.jl:475-524, src/DEER/DEER.jl:506-595): draws the tape of
+ * (seed, block), solves the T-step trajectory from x0 and writes
+ *   S_out    D x T trajectory (dtype), column t = x_{t+1}
+ *   logp_out T log densities of the returned columns (dtype), may be NULL
+ *   accept_out T accept flags (uint8), may be NULL
+ * x0 has dtype and lives in `mem`; outputs live in `mem`. */
+int pmcmc_deer_solve(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                     const void* x0, uint64_t seed, uint64_t block, void* S_out, void* logp_out,
+                     uint8_t* accept_out, int32_t mem, pmcmc_info* info);
+
+/* ---- block loop ---------------------------------------------------------------
+ * Replaces the block loop of _sample_parallel_mala_chain / _blocks
+ * (src/interface.jl:557-607, 661-711): ceil(N/T) blocks, block b uses tape
+ * block b, keeps min(T, N - nsteps) columns, next x0 = last kept column.
+ * vals_out D x N (dtype), logp_out N (dtype, may be NULL), accept_out N (may be NULL).
+ * info accumulates: iters = total sweeps, converged = all blocks converged,
+ * metric = worst block metric. */
+int pmcmc_sample(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                 const void* x0, uint64_t seed, int64_t N, void* vals_out, void* logp_out,
+                 uint8_t* accept_out, int32_t mem, pmcmc_info* info);
+
+/* ---- diagonal affine scan ----------------------------------------------------
+ * Replaces DEERScan.solve_affine_scan_diag! (src/DEER/DEERScan.jl:102-173):
+ * S[:,t] = A[:,t] .* S[:,t-1] + B[:,t], S[:,0-1] = s0.  Single-pass
+ * decoupled-lookback scan.  S may not alias A or B (DEERScan.jl:124-125). */
+int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T, const void* A,
+                           const void* B, const void* s0, void* S, int32_t mem);
+
+/* ---- profiling ------------------------------------------------------------
+ * With profiling on, solves run their Newton loop as individual launches with
+ * CUDA events around every sweep and finalize kernel (no graph); the device
+ * times accumulate until pmcmc_get_profile is called with reset = 1.  Used by
+ * bench.py to time the dominant kernel; no counterpart in the reference
+ * (its benchmarks time whole solves, benchmarks/.../profile_deer_logreg_components.jl). */
+typedef struct {
+  int64_t sweep_launches;
+  double sweep_ms;
+  int64_t finalize_launches;
+  double finalize_ms;
+} pmcmc_profile;
+int pmcmc_set_profiling(pmcmc_handle* h, int32_t on);
+int pmcmc_get_profile(pmcmc_handle* h, pmcmc_profile* out, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMCMC_DEER_H */

@@ -1,0 +1,192 @@
+// deer_device.cuh -- device-resident solve parameters/state and the shared
+// building blocks of the DEER sweep: warp reductions, tile-local affine scan
+// and the decoupled look-back across tiles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pmcmc_rng.cuh"
+
+namespace pmcmc {
+
+constexpr int kThreads = 256;  // threads per CTA of the sweep / scan kernels
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kFlagAgg = 1u, kFlagIncl = 2u;
+constexpr long long kMaxSpins = 1ll << 22;  // bounded look-back wait (~0.3 s), then error
+
+enum TargetKind : int32_t { kDiagGauss = 0, kDenseGauss = 1, kLogistic = 2 };
+enum JacKind : int32_t { kJacStoch = 0, kJacDiag = 1, kJacFull = 2 };
+enum DevStatus : int32_t { kStOk = 0, kStNonfinite = 4, kStTimeout = 5 };
+
+// Everything a solve needs, resident in device memory so that one captured
+// CUDA graph serves every call (kernels copy it to shared memory on entry).
+struct DevParams {
+  int64_t D, Dp, T, W;  // Dp = D rounded up to 4; W = window width (T if none)
+  int64_t ncols_out;    // columns copied to S_out by the finalize pass
+  double eps, sqrt2eps, inv4eps, inv2eps, damping, tol_abs, tol_rel;
+  uint64_t seed, block;
+  int32_t jac, probes, maxiter, tile_cols;
+  int32_t ntiles, tkind, out_device, pad0;
+  // target (device copies, both precisions)
+  const double* mean_d;
+  const double* prec_d;
+  const float* mean_f;
+  const float* prec_f;
+  // trajectory ping-pong buffers and start state (Real)
+  void* S[2];
+  const void* x0;
+  // look-back scratch
+  uint32_t* flags;  // [ntiles]
+  void* agg_a;      // [ntiles * Dp]
+  void* agg_b;
+  void* incl;
+  float* colmax;  // [T] per-column max |dS| (window mode)
+  // outputs
+  void* S_out;
+  void* logp_out;
+  uint8_t* accept_out;
+  void* x_next;  // [D] last kept column (next block's x0)
+};
+
+struct DevState {
+  int32_t iter, cur, converged, status;
+  int64_t t_lo, t_lo_prev;
+  uint32_t epoch, tile_counter, done_counter, fin_counter;
+  unsigned long long dmax_bits, smax_bits;  // non-negative doubles as ordered bits
+  double metric;
+  unsigned long long n_accept;
+  unsigned long long min_margin_bits, max_defect_bits;
+};
+
+__host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long dbits(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double(static_cast<long long>(b));
+}
+
+// Inclusive scan of the affine maps x -> A[c][d] x + B[c][d] along c (columns
+// 0..ncols-1 of a tile), independently for every coordinate d, in place.
+// After the call (A[c][d], B[c][d]) is the composition of columns 0..c.
+// Threads own (d, chunk) pairs: a serial scan inside each chunk, then each
+// chunk is offset by the composition of the chunks before it.
+template <typename Real>
+__device__ void tile_scan_inplace(Real* As, Real* Bs, int ncols, int D, int Dp) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (ncols <= 0) return;
+  int C = D >= nt ? 1 : min(nt / D, ncols);
+  const int L = (ncols + C - 1) / C;
+  C = (ncols + L - 1) / L;
+  for (int base = 0; base < D * C; base += nt) {
+    const int k = base + tid;
+    if (k < D * C) {
+      const int d = k % D, ch = k / D;
+      const int c0 = ch * L, c1 = min(ncols, c0 + L);
+      Real a = As[c0 * Dp + d], b = Bs[c0 * Dp + d];
+      for (int c = c0 + 1; c < c1; ++c) {
+        const Real ac = As[c * Dp + d], bc = Bs[c * Dp + d];
+        b = ac * b + bc;
+        a = ac * a;
+        As[c * Dp + d] = a;
+        Bs[c * Dp + d] = b;
+      }
+    }
+  }
+  if (C == 1) return;
+  __syncthreads();
+  // Exclusive prefix of each chunk from the chunk aggregates (read first, then apply).
+  Real ea[4], eb[4];  // up to 4 (d, chunk) items per thread when D*C > nt
+  int nitems = 0;
+  for (int base = 0; base < D * C; base += nt, ++nitems) {
+    const int k = base + tid;
+    Real a = 1, b = 0;
+    if (k < D * C) {
+      const int d = k % D, ch = k / D;
+      for (int j = 0; j < ch; ++j) {
+        const int e = min(ncols, (j + 1) * L) - 1;
+        const Real aj = As[e * Dp + d], bj = Bs[e * Dp + d];
+        b = aj * b + bj;
+        a = aj * a;
+      }
+    }
+    if (nitems < 4) {
+      ea[nitems] = a;
+      eb[nitems] = b;
+    }
+  }
+  __syncthreads();
+  nitems = 0;
+  for (int base = 0; base < D * C; base += nt, ++nitems) {
+    const int k = base + tid;
+    if (k < D * C && nitems < 4) {
+      const int d = k % D, ch = k / D;
+      if (ch == 0) continue;
+      const int c0 = ch * L, c1 = min(ncols, c0 + L);
+      for (int c = c0; c < c1; ++c) {
+        const Real ac = As[c * Dp + d];
+        Bs[c * Dp + d] = ac * eb[nitems] + Bs[c * Dp + d];
+        As[c * Dp + d] = ac * ea[nitems];
+      }
+    }
+  }
+}
+
+// Decoupled look-back (Merrill & Garland) over per-coordinate affine maps:
+// returns the state entering tile `tile` for coordinate d.  Waits are bounded:
+// after kMaxSpins polls the error flag is set and the call returns.
+template <typename Real>
+__device__ Real lookback_state(int tile, int d, int Dp, uint32_t epoch, const uint32_t* flags,
+                               const Real* agg_a, const Real* agg_b, const Real* incl,
+                               Real s_lo, int* err) {
+  Real a = 1, b = 0;
+  for (int j = tile - 1; j >= 0; --j) {
+    uint32_t f = 0;
+    long long spins = 0;
+    while (true) {
+      f = ld_acquire(flags + j);
+      if ((f >> 2) == (epoch & 0x3fffffffu) && (f & 3u)) break;
+      if (++spins > kMaxSpins) {
+        *err = 1;
+        return Real(0);
+      }
+      __nanosleep(64);
+    }
+    if ((f & 3u) == kFlagIncl) {
+      const Real s = __ldcg(incl + static_cast<size_t>(j) * Dp + d);
+      return a * s + b;
+    }
+    const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
+    const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
+    b = a * bj + b;
+    a = a * aj;
+  }
+  return a * s_lo + b;
+}
+
+}  // namespace pmcmc

@@ -1,0 +1,58 @@
+// deer_launch.h -- host-side view of the kernels (no torch types, plain CUDA runtime).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace pmcmc {
+
+struct SmemPlan {
+  size_t xs, as, carry, pd, pf, vd, vf, total;
+  int p_in_smem;
+};
+
+struct SweepKernels {
+  const void* sweep = nullptr;     // (const DevParams*, DevState*, cudaGraphConditionalHandle, int)
+  const void* finalize = nullptr;  // (const DevParams*, DevState*)
+  const void* init = nullptr;      // (const DevParams*, DevState*)
+  const void* eval = nullptr;      // (const DevParams*, const Real* Sold, int iter, int from_x0, Real* A, Real* B)
+  int qpl = 1;
+};
+
+SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D);
+SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);
+
+// Tape materialisation (tape.cu).
+cudaError_t launch_tape(cudaStream_t s, int64_t D, int64_t T, uint64_t seed, uint64_t block,
+                        float* Xi, float* u);
+
+// Standalone diagonal affine scan (scan_diag.cu).  Scratch: flags[ntiles],
+// agg_a/agg_b/incl[ntiles * Dp] of the element type, counter[1].
+struct ScanScratch {
+  uint32_t* flags;
+  void* agg_a;
+  void* agg_b;
+  void* incl;
+  uint32_t* counter;
+};
+int scan_tile_cols(int64_t D, int64_t T);
+size_t scan_scratch_bytes(bool f64, int64_t D, int64_t T);
+cudaError_t launch_affine_scan(cudaStream_t s, bool f64, int64_t D, int64_t T, const void* A,
+                               const void* B, const void* s0, void* S, const ScanScratch& scr,
+                               uint32_t epoch);
+
+// Plain path (tape_scan.cu): the reference's Hillis-Steele doubling scan
+// (DEERScan.jl:102-173) as one launch per level over buffers of T x Dp
+// elements, and damping + max-reductions into red[2] (double bits).
+cudaError_t launch_doubling_scan(cudaStream_t s, bool f64, int64_t Dp, int64_t T, const void* A,
+                                 const void* B, const void* s0, void* S, void* al0, void* be0,
+                                 void* al1, void* be1);
+cudaError_t launch_damp_metric(cudaStream_t s, bool f64, int64_t D, int64_t Dp, int64_t T,
+                               const void* S_old, void* S_new, double damping,
+                               unsigned long long* red);
+
+cudaError_t launch_broadcast(cudaStream_t s, bool f64, int64_t Dp, int64_t T, const void* x0,
+                             void* S);
+
+}  // namespace pmcmc

@@ -1,0 +1,941 @@
+// deer_sweep.cu -- fused Newton sweep for the Gaussian device targets.
+//
+// One launch = one DEER iteration over the whole block (DEER.jl:553-581):
+//   x_bar_t = S_{t-1} (x0 for t = 0)                       DEER.jl:402-405
+//   MALA proposal, FP64 log-acceptance, forward step        MALA.jl:577-597
+//   Jacobian diagonal: Hutchinson probes (MALA.jl:599-625, DEER.jl:407-418)
+//     or the exact diagonal (jac_diag_via_jvps, DEER.jl:327-342) in closed form
+//   B = F - A .* x_bar                                      DEER.jl:419
+//   S_t = A_t .* S_{t-1} + B_t                              DEERScan.jl:102-173
+//   damping, max|dS| and max|S| in FP64                     DEER.jl:471-473, 567-571
+// Each CTA owns a tile of consecutive columns: it stages S_old (plus one halo
+// column) in shared memory, evaluates the tile, scans it locally and joins its
+// predecessors through a decoupled look-back, then writes S_new once.  The
+// tape (xi, u) and the probes are regenerated in registers, so a sweep reads
+// and writes the trajectory once.  The last CTA to finish evaluates the
+// convergence test and drives the CUDA-graph while-node.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "deer_device.cuh"
+#include "deer_launch.h"
+
+namespace pmcmc {
+
+template <typename Real>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using T = float4;
+};
+template <>
+struct Vec4<double> {
+  using T = double4;
+};
+
+template <typename Real>
+__device__ __forceinline__ void load4(const Real* p, Real v[4]) {
+  const auto q = *reinterpret_cast<const typename Vec4<Real>::T*>(p);
+  v[0] = q.x;
+  v[1] = q.y;
+  v[2] = q.z;
+  v[3] = q.w;
+}
+template <typename Real>
+__device__ __forceinline__ void store4(Real* p, const Real v[4]) {
+  typename Vec4<Real>::T q;
+  q.x = v[0];
+  q.y = v[1];
+  q.z = v[2];
+  q.w = v[3];
+  *reinterpret_cast<typename Vec4<Real>::T*>(p) = q;
+}
+
+template <typename Real>
+__device__ __forceinline__ const Real* prec_of(const DevParams& P);
+template <>
+__device__ __forceinline__ const float* prec_of<float>(const DevParams& P) {
+  return P.prec_f;
+}
+template <>
+__device__ __forceinline__ const double* prec_of<double>(const DevParams& P) {
+  return P.prec_d;
+}
+template <typename Real>
+__device__ __forceinline__ const Real* mean_of(const DevParams& P);
+template <>
+__device__ __forceinline__ const float* mean_of<float>(const DevParams& P) {
+  return P.mean_f;
+}
+template <>
+__device__ __forceinline__ const double* mean_of<double>(const DevParams& P) {
+  return P.mean_d;
+}
+
+// out[e] = sum_k M(4j+e, k) v[k]; M column-major, leading dimension Dp,
+// padded rows zero; v is a warp-private vector in shared memory.
+template <typename M, typename V, typename Acc>
+__device__ __forceinline__ void matvec4(const M* __restrict__ Mm, const V* v, int D, int Dp,
+                                        int j, Acc out[4]) {
+  Acc a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  const M* col = Mm + 4 * j;
+  for (int k = 0; k < D; ++k) {
+    const Acc vk = static_cast<Acc>(v[k]);
+    M m[4];
+    load4(col + static_cast<size_t>(k) * Dp, m);
+    a0 = fma(static_cast<Acc>(m[0]), vk, a0);
+    a1 = fma(static_cast<Acc>(m[1]), vk, a1);
+    a2 = fma(static_cast<Acc>(m[2]), vk, a2);
+    a3 = fma(static_cast<Acc>(m[3]), vk, a3);
+  }
+  out[0] = a0;
+  out[1] = a1;
+  out[2] = a2;
+  out[3] = a3;
+}
+
+// ---------------------------------------------------------------------------
+// Shared memory
+// ---------------------------------------------------------------------------
+template <typename Real>
+struct Smem {
+  Real* Xs;     // (TT+1) x Dp : S_old columns t0-1 .. t0+TT-1
+  Real* As;     // TT x Dp
+  Real* Bs;     // TT x Dp
+  Real* carry;  // Dp
+  const double* Pd;  // dense precision in double (smem copy or global)
+  const Real* Pf;    // dense precision in Real
+  double* Vd;        // kWarps x Dp warp-private vectors
+  Real* Vf;          // kWarps x Dp
+};
+
+template <typename Real>
+__host__ __device__ inline SmemPlan plan_sweep_smem(int64_t Dp, int TT, bool dense) {
+  SmemPlan s{};
+  size_t off = 0;
+  auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+  s.xs = off;
+  off = al(off + sizeof(Real) * (TT + 1) * Dp);
+  s.as = off;
+  off = al(off + sizeof(Real) * 2 * TT * Dp);
+  s.carry = off;
+  off = al(off + sizeof(Real) * Dp);
+  s.p_in_smem = 0;
+  if (dense) {
+    s.vd = off;
+    off = al(off + sizeof(double) * kWarps * Dp);
+    s.vf = off;
+    off = al(off + sizeof(Real) * kWarps * Dp);
+    const size_t pbytes = (sizeof(double) + sizeof(Real)) * Dp * Dp + 32;
+    if (off + pbytes <= 150 * 1024) {
+      s.p_in_smem = 1;
+      s.pd = off;
+      off = al(off + sizeof(double) * Dp * Dp);
+      s.pf = off;
+      off = al(off + sizeof(Real) * Dp * Dp);
+    }
+  }
+  s.total = off;
+  return s;
+}
+
+template <typename Real>
+__device__ Smem<Real> carve(unsigned char* base, const DevParams& P, int TT, bool dense) {
+  const SmemPlan pl = plan_sweep_smem<Real>(P.Dp, TT, dense);
+  Smem<Real> s;
+  s.Xs = reinterpret_cast<Real*>(base + pl.xs);
+  s.As = reinterpret_cast<Real*>(base + pl.as);
+  s.Bs = s.As + static_cast<size_t>(TT) * P.Dp;
+  s.carry = reinterpret_cast<Real*>(base + pl.carry);
+  s.Vd = nullptr;
+  s.Vf = nullptr;
+  s.Pd = P.prec_d;
+  s.Pf = prec_of<Real>(P);
+  if (dense) {
+    s.Vd = reinterpret_cast<double*>(base + pl.vd);
+    s.Vf = reinterpret_cast<Real*>(base + pl.vf);
+    const int nv = static_cast<int>(kWarps * P.Dp);
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+      s.Vd[i] = 0.0;
+      s.Vf[i] = Real(0);
+    }
+    if (pl.p_in_smem) {
+      double* pd = reinterpret_cast<double*>(base + pl.pd);
+      Real* pf = reinterpret_cast<Real*>(base + pl.pf);
+      const int n = static_cast<int>(P.Dp * P.Dp);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        pd[i] = P.prec_d[i];
+        pf[i] = prec_of<Real>(P)[i];
+      }
+      s.Pd = pd;
+      s.Pf = pf;
+    }
+  }
+  return s;
+}
+
+__device__ __forceinline__ void load_params(const DevParams* Pg, DevParams& sp) {
+  constexpr int n = sizeof(DevParams) / sizeof(unsigned long long);
+  static_assert(sizeof(DevParams) % sizeof(unsigned long long) == 0, "DevParams padding");
+  if (threadIdx.x < n)
+    reinterpret_cast<unsigned long long*>(&sp)[threadIdx.x] =
+        reinterpret_cast<const unsigned long long*>(Pg)[threadIdx.x];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// One column, one warp.  Lane owns quads j = lane + 32 q (d = 4j .. 4j+3).
+// ---------------------------------------------------------------------------
+template <typename Real, int QPL>
+struct Col {
+  Real x[QPL][4], xi[QPL][4], gx[QPL][4], y[QPL][4], gy[QPL][4];
+  double la;
+};
+
+// Forward MALA half (MALA.jl:577-592): gradient, proposal y (Real), gradient
+// at y, and the FP64 log acceptance ratio.  The D/2 log(4 pi eps) constants of
+// the two logq terms cancel exactly and are not formed; y - x - eps g_x is
+// sqrt(2 eps) xi by construction of y.
+template <typename Real, int TK, int QPL>
+__device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Real>& sm,
+                                               const TapeKey& key, const Real* xcol, int t,
+                                               Col<Real, QPL>& c) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  const Real eps = static_cast<Real>(P.eps), c2 = static_cast<Real>(P.sqrt2eps);
+  double la = 0.0;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < D) {
+      load4(xcol + 4 * j, c.x[q]);
+      float n[4];
+      tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), n);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) c.xi[q][e] = static_cast<Real>(n[e]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) c.x[q][e] = c.xi[q][e] = Real(0);
+    }
+  }
+  if constexpr (TK == kDiagGauss) {
+    const Real* lamR = prec_of<Real>(P);
+    const Real* muR = mean_of<Real>(P);
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        Real lam[4], mu[4];
+        double lamd[4], mud[4];
+        load4(lamR + 4 * j, lam);
+        load4(muR + 4 * j, mu);
+        load4(P.prec_d + 4 * j, lamd);
+        load4(P.mean_d + 4 * j, mud);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const Real gx = -lam[e] * (c.x[q][e] - mu[e]);
+          const Real y = fma(c2, c.xi[q][e], fma(eps, gx, c.x[q][e]));
+          c.gx[q][e] = gx;
+          c.y[q][e] = y;
+          c.gy[q][e] = -lam[e] * (y - mu[e]);
+          if (4 * j + e < D) {
+            const double xd = static_cast<double>(c.x[q][e]) - mud[e];
+            const double yd = static_cast<double>(y) - mud[e];
+            const double lp = -0.5 * lamd[e] * (yd * yd - xd * xd);
+            const double r1 = P.sqrt2eps * static_cast<double>(c.xi[q][e]);
+            const double r2 = (static_cast<double>(c.x[q][e]) - static_cast<double>(y)) +
+                              P.eps * lamd[e] * yd;
+            la += lp + (r1 * r1 - r2 * r2) * P.inv4eps;
+          }
+        }
+      }
+    }
+  } else {
+    // Dense Gaussian: gradients in FP64 through warp-private shared vectors.
+    double* vd = sm.Vd + warp * Dp;
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * j + e < D) vd[4 * j + e] = static_cast<double>(c.x[q][e]) - P.mean_d[4 * j + e];
+    }
+    __syncwarp();
+    double gxd[QPL][4];
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        double o[4];
+        matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          gxd[q][e] = -o[e];
+          c.gx[q][e] = static_cast<Real>(-o[e]);
+          c.y[q][e] = fma(c2, c.xi[q][e], fma(eps, c.gx[q][e], c.x[q][e]));
+          if (4 * j + e < D)
+            la -= 0.5 * (static_cast<double>(c.x[q][e]) - P.mean_d[4 * j + e]) * gxd[q][e];
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) gxd[q][e] = 0.0, c.gx[q][e] = c.y[q][e] = Real(0);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * j + e < D) vd[4 * j + e] = static_cast<double>(c.y[q][e]) - P.mean_d[4 * j + e];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        double o[4];
+        matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          c.gy[q][e] = static_cast<Real>(-o[e]);
+          if (4 * j + e < D) {
+            const double yd = static_cast<double>(c.y[q][e]) - P.mean_d[4 * j + e];
+            la += 0.5 * yd * (-o[e]);
+            const double r1 = P.sqrt2eps * static_cast<double>(c.xi[q][e]);
+            const double r2 = (static_cast<double>(c.x[q][e]) - static_cast<double>(c.y[q][e])) +
+                              P.eps * o[e];
+            la += (r1 * r1 - r2 * r2) * P.inv4eps;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) c.gy[q][e] = Real(0);
+      }
+    }
+    __syncwarp();
+  }
+  c.la = warp_sum(la);
+}
+
+// Dense HVP quad: out = -P v (v written to the warp's Real vector first).
+template <typename Real, int QPL>
+__device__ __forceinline__ void dense_neg_pv(const DevParams& P, const Smem<Real>& sm,
+                                             const Real (&v)[QPL][4], Real (&out)[QPL][4]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  Real* vf = sm.Vf + warp * Dp;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < D)
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * j + e < D) vf[4 * j + e] = v[q][e];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < D) {
+      Real o[4];
+      matvec4<Real, Real, Real>(sm.Pf, vf, D, Dp, j, o);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) out[q][e] = -o[e];
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) out[q][e] = Real(0);
+    }
+  }
+  __syncwarp();
+}
+
+// Jacobian diagonal estimate A (Real) for one evaluated column.
+template <typename Real, int TK, int JAC, int QPL>
+__device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<Real>& sm,
+                                                const TapeKey& key, int t, int iter, bool acc,
+                                                Real gp, const Col<Real, QPL>& c,
+                                                Real (&A)[QPL][4]) {
+  const int lane = threadIdx.x & 31;
+  const int D = static_cast<int>(P.D);
+  const Real eps = static_cast<Real>(P.eps), inv2eps = static_cast<Real>(P.inv2eps);
+  const Real* lamR = prec_of<Real>(P);
+  if constexpr (JAC == kJacStoch) {
+#pragma unroll
+    for (int q = 0; q < QPL; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) A[q][e] = Real(0);
+    for (int k = 0; k < P.probes; ++k) {
+      Real z[QPL][4], w[QPL][4], hvy[QPL][4];
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+        if (4 * j < D) {
+          const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t),
+                                   k, iter);
+          const uint32_t wv = u4_word(pb, (j >> 3) & 3);
+          const int sh = (j & 7) * 4;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) z[q][e] = ((wv >> (sh + e)) & 1u) ? Real(1) : Real(-1);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) z[q][e] = Real(0);
+        }
+      }
+      if constexpr (TK == kDiagGauss) {
+#pragma unroll
+        for (int q = 0; q < QPL; ++q) {
+          const int j = lane + 32 * q;
+          Real lam[4] = {0, 0, 0, 0};
+          if (4 * j < D) load4(lamR + 4 * j, lam);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            w[q][e] = z[q][e] + eps * (-lam[e] * z[q][e]);
+            hvy[q][e] = -lam[e] * w[q][e];
+          }
+        }
+      } else {
+        Real hvx[QPL][4];
+        dense_neg_pv<Real, QPL>(P, sm, z, hvx);
+#pragma unroll
+        for (int q = 0; q < QPL; ++q)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) w[q][e] = z[q][e] + eps * hvx[q][e];
+        dense_neg_pv<Real, QPL>(P, sm, w, hvy);
+      }
+      Real dla = 0;
+#pragma unroll
+      for (int q = 0; q < QPL; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const Real r = c.x[q][e] - c.y[q][e] - eps * c.gy[q][e];
+          const Real dr = z[q][e] - w[q][e] - eps * hvy[q][e];
+          dla += c.gy[q][e] * w[q][e] - c.gx[q][e] * z[q][e] - inv2eps * r * dr;
+        }
+      dla = warp_sum(dla);
+      const Real dg = gp * dla;
+#pragma unroll
+      for (int q = 0; q < QPL; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const Real jz = (acc ? w[q][e] : z[q][e]) + (c.y[q][e] - c.x[q][e]) * dg;
+          A[q][e] += z[q][e] * jz;
+        }
+    }
+    if (P.probes > 1) {
+      const Real inv = Real(1) / static_cast<Real>(P.probes);
+#pragma unroll
+      for (int q = 0; q < QPL; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) A[q][e] *= inv;
+    }
+  } else {
+    // Exact diagonal: (J e_i)_i = a (1 + eps H_ii) + (1 - a) + (y_i - x_i) g(1-g) dlogalpha(e_i),
+    // dlogalpha(e_i) = [(I + eps H) g_y]_i - g_x,i + 1/2 ([H r]_i + [H r]_i + eps [H H r]_i).
+    if constexpr (TK == kDiagGauss) {
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+        Real lam[4] = {0, 0, 0, 0};
+        if (4 * j < D) load4(lamR + 4 * j, lam);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const Real el = eps * lam[e];
+          const Real r = c.x[q][e] - c.y[q][e] - eps * c.gy[q][e];
+          const Real dl = (Real(1) - el) * c.gy[q][e] - c.gx[q][e] -
+                          lam[e] * r * (Real(1) - Real(0.5) * el);
+          A[q][e] = (acc ? Real(1) - el : Real(1)) + (c.y[q][e] - c.x[q][e]) * gp * dl;
+        }
+      }
+    } else {
+      Real r[QPL][4], pgy[QPL][4], pr[QPL][4], ppr[QPL][4];
+#pragma unroll
+      for (int q = 0; q < QPL; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) r[q][e] = c.x[q][e] - c.y[q][e] - eps * c.gy[q][e];
+      dense_neg_pv<Real, QPL>(P, sm, c.gy, pgy);  // -P g_y
+      dense_neg_pv<Real, QPL>(P, sm, r, pr);      // -P r
+      dense_neg_pv<Real, QPL>(P, sm, pr, ppr);    // P P r
+      const int Dp = static_cast<int>(P.Dp);
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int i = 4 * j + e;
+          const Real pii = i < D ? sm.Pf[static_cast<size_t>(i) * Dp + i] : Real(0);
+          const Real dl = c.gy[q][e] + eps * pgy[q][e] - c.gx[q][e] + pr[q][e] +
+                          Real(0.5) * eps * ppr[q][e];
+          A[q][e] = (acc ? Real(1) - eps * pii : Real(1)) + (c.y[q][e] - c.x[q][e]) * gp * dl;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The sweep kernel
+// ---------------------------------------------------------------------------
+template <typename Real, int TK, int JAC, int QPL>
+__global__ void __launch_bounds__(kThreads)
+    deer_sweep_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st,
+                      cudaGraphConditionalHandle cond, int use_cond) {
+  __shared__ DevParams P;
+  __shared__ int s_tile, s_last, s_err, s_nonfinite;
+  __shared__ double s_red[2][kWarps];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  load_params(Pg, P);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int32_t iter = *reinterpret_cast<volatile int32_t*>(&st->iter);
+  if (!use_cond) {
+    // eager mode: extra launches after convergence are no-ops
+    if (*reinterpret_cast<volatile int32_t*>(&st->converged) || iter >= P.maxiter ||
+        *reinterpret_cast<volatile int32_t*>(&st->status) != 0)
+      return;
+  }
+  const int cur = *reinterpret_cast<volatile int32_t*>(&st->cur);
+  const int64_t t_lo = *reinterpret_cast<volatile int64_t*>(&st->t_lo);
+  const int64_t t_lo_prev = *reinterpret_cast<volatile int64_t*>(&st->t_lo_prev);
+  const uint32_t epoch = *reinterpret_cast<volatile uint32_t*>(&st->epoch);
+  if (tid == 0) {
+    s_tile = static_cast<int>(atomicAdd(&st->tile_counter, 1u));
+    s_err = 0;
+    s_nonfinite = 0;
+  }
+  __syncthreads();
+  const int tile = s_tile;
+  const int TT = P.tile_cols;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  const int64_t T = P.T;
+  const bool windowed = P.W < T;
+  const int64_t t_hi = min(T, t_lo + P.W);
+  const int64_t t0 = t_lo + static_cast<int64_t>(tile) * TT;
+  const int64_t rem = t_hi - t0;
+  const int ncols = rem <= 0 ? 0 : static_cast<int>(rem < TT ? rem : TT);
+  const Real* Sold = static_cast<const Real*>(P.S[cur]);
+  Real* Snew = static_cast<Real*>(P.S[cur ^ 1]);
+  const Real* x0 = static_cast<const Real*>(P.x0);
+  const bool from_x0 = (!windowed) && iter == 0;  // first sweep: S_old = s0 broadcast
+
+  // Window mode: columns finalised by the previous sweep are copied into the
+  // buffer this sweep writes, so both buffers agree on every final column.
+  if (windowed && t_lo > t_lo_prev) {
+    const int64_t n = (t_lo - t_lo_prev) * Dp;
+    for (int64_t i = static_cast<int64_t>(tile) * kThreads + tid; i < n;
+         i += static_cast<int64_t>(gridDim.x) * kThreads)
+      Snew[t_lo_prev * Dp + i] = Sold[t_lo_prev * Dp + i];
+  }
+
+  Smem<Real> sm = carve<Real>(smem_raw, P, TT, TK == kDenseGauss);
+  double my_dmax = 0.0, my_smax = 0.0;
+
+  if (ncols > 0) {
+    // ---- stage S_old columns t0-1 .. t0+ncols-1 ----
+    const int nstage = (ncols + 1) * Dp;
+    for (int i = tid; i < nstage; i += kThreads) {
+      const int c = i / Dp;
+      const int64_t t = t0 - 1 + c;
+      Real v;
+      if (from_x0 || t < 0) v = x0[i - c * Dp];
+      else if (t < t_lo) v = Sold[(t_lo - 1) * Dp + (i - c * Dp)];  // s_{t_lo - 1}
+      else v = Sold[t * Dp + (i - c * Dp)];
+      sm.Xs[i] = v;
+    }
+    __syncthreads();
+
+    // ---- phase 1: evaluate columns (one warp per column) ----
+    const TapeKey key(P.seed, P.block);
+    for (int c = warp; c < ncols; c += kWarps) {
+      const int t = static_cast<int>(t0 + c);
+      Col<Real, QPL> col;
+      column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col);
+      const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+      const bool acc = logu < col.la;
+      const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
+      const Real gp = static_cast<Real>(gd * (1.0 - gd));
+      Real A[QPL][4];
+      column_jacobian<Real, TK, JAC, QPL>(P, sm, key, t, iter, acc, gp, col, A);
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+        if (4 * j < D) {
+          Real a4[4], b4[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const Real f = acc ? col.y[q][e] : col.x[q][e];
+            a4[e] = (4 * j + e < D) ? A[q][e] : Real(0);
+            b4[e] = (4 * j + e < D) ? f - A[q][e] * col.x[q][e] : Real(0);
+          }
+          store4(sm.As + c * Dp + 4 * j, a4);
+          store4(sm.Bs + c * Dp + 4 * j, b4);
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- phase 2: tile-local inclusive scan ----
+    tile_scan_inplace<Real>(sm.As, sm.Bs, ncols, D, Dp);
+    __syncthreads();
+
+    // ---- phase 3: decoupled look-back for the state entering the tile ----
+    Real* agg_a = static_cast<Real*>(P.agg_a);
+    Real* agg_b = static_cast<Real*>(P.agg_b);
+    Real* incl = static_cast<Real*>(P.incl);
+    const size_t last = static_cast<size_t>(ncols - 1) * Dp;
+    if (tile == 0) {
+      for (int d = tid; d < D; d += kThreads) {
+        const Real s_lo = sm.Xs[d];
+        sm.carry[d] = s_lo;
+        incl[d] = sm.As[last + d] * s_lo + sm.Bs[last + d];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(P.flags, (epoch << 2) | kFlagIncl);
+    } else {
+      for (int d = tid; d < D; d += kThreads) {
+        agg_a[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d];
+        agg_b[static_cast<size_t>(tile) * Dp + d] = sm.Bs[last + d];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagAgg);
+      int err = 0;
+      for (int d = tid; d < D; d += kThreads) {
+        const Real cin = lookback_state<Real>(tile, d, Dp, epoch, P.flags, agg_a, agg_b, incl,
+                                              sm.Xs[d], &err);
+        sm.carry[d] = cin;
+        incl[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d] * cin + sm.Bs[last + d];
+      }
+      if (err) s_err = 1;
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagIncl);
+    }
+    __syncthreads();
+
+    // ---- phase 4: apply carry, damping, metric, write S_new ----
+    const Real dmp = static_cast<Real>(P.damping), omd = static_cast<Real>(1.0 - P.damping);
+    const bool undamped = P.damping == 1.0;
+    Real cr[QPL][4];
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) load4(sm.carry + 4 * j, cr[q]);
+    }
+    bool bad = false;
+    for (int c = warp; c < ncols; c += kWarps) {
+      const int64_t t = t0 + c;
+      Real cmax = 0;
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+        if (4 * j < D) {
+          Real a4[4], b4[4], o4[4], n4[4];
+          load4(sm.As + c * Dp + 4 * j, a4);
+          load4(sm.Bs + c * Dp + 4 * j, b4);
+          load4(sm.Xs + (c + 1) * Dp + 4 * j, o4);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const Real s = a4[e] * cr[q][e] + b4[e];
+            n4[e] = undamped ? s : omd * o4[e] + dmp * s;
+            if (4 * j + e < D) {
+              const Real dv = fabs(n4[e] - o4[e]);
+              cmax = max(cmax, dv);
+              my_dmax = max(my_dmax, static_cast<double>(dv));
+              my_smax = max(my_smax, static_cast<double>(fabs(n4[e])));
+              bad |= !isfinite(n4[e]);
+            } else {
+              n4[e] = Real(0);
+            }
+          }
+          store4(Snew + t * Dp + 4 * j, n4);
+        }
+      }
+      if (windowed) {
+        cmax = warp_max(cmax);
+        if (lane == 0) P.colmax[t] = static_cast<float>(cmax);
+      }
+    }
+    if (bad) s_nonfinite = 1;
+  }
+
+  // ---- block reduction of the metric, one atomic per CTA ----
+  my_dmax = warp_max(my_dmax);
+  my_smax = warp_max(my_smax);
+  if (lane == 0) {
+    s_red[0][warp] = my_dmax;
+    s_red[1][warp] = my_smax;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < kWarps; ++w) a = max(a, s_red[0][w]), b = max(b, s_red[1][w]);
+    if (a > 0) atomicMax(&st->dmax_bits, dbits(a));
+    if (b > 0) atomicMax(&st->smax_bits, dbits(b));
+    if (s_err) atomicExch(&st->status, static_cast<int>(kStTimeout));
+    if (s_nonfinite) atomicCAS(&st->status, 0, static_cast<int>(kStNonfinite));
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->done_counter, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+
+  // ---- last CTA: convergence test (DEER.jl:567-578) and loop control ----
+  __threadfence();
+  const double dmax = bitsd(atomicAdd(&st->dmax_bits, 0ull));
+  const double smax = bitsd(atomicAdd(&st->smax_bits, 0ull));
+  const double scale = P.tol_abs + P.tol_rel * smax;
+  const double metric = dmax / scale;
+  int64_t new_t_lo = t_lo;
+  if (windowed) {
+    // t_lo advances to the first column whose change exceeds the scale.
+    __shared__ long long s_first;
+    if (tid == 0) s_first = t_hi;
+    __syncthreads();
+    long long mine = t_hi;
+    for (int64_t t = t_lo + tid; t < t_hi; t += kThreads)
+      if (static_cast<double>(__ldcg(P.colmax + t)) > scale) {
+        mine = t;
+        break;
+      }
+    atomicMin(&s_first, mine);
+    __syncthreads();
+    new_t_lo = s_first;
+  }
+  if (tid == 0) {
+    const int status = atomicAdd(&st->status, 0);
+    const int converged = windowed ? (new_t_lo >= T) : (metric <= 1.0);
+    st->metric = metric;
+    st->iter = iter + 1;
+    st->cur = cur ^ 1;
+    st->t_lo_prev = t_lo;
+    st->t_lo = new_t_lo;
+    st->converged = converged;
+    st->epoch = epoch + 1;
+    st->tile_counter = 0;
+    st->done_counter = 0;
+    st->dmax_bits = 0;
+    st->smax_bits = 0;
+    __threadfence();
+    const bool more = !converged && (iter + 1 < P.maxiter) && status == 0;
+    if (use_cond) cudaGraphSetConditional(cond, more ? 1u : 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reset of the per-solve device state (and, in window mode, both buffers).
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void deer_init_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st) {
+  const DevParams& P = *Pg;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = 0;
+    st->cur = 0;
+    st->converged = 0;
+    st->status = 0;
+    st->t_lo = 0;
+    st->t_lo_prev = 0;
+    st->epoch = st->epoch + 1;
+    st->tile_counter = 0;
+    st->done_counter = 0;
+    st->fin_counter = 0;
+    st->dmax_bits = 0;
+    st->smax_bits = 0;
+    st->metric = __longlong_as_double(0x7ff0000000000000ll);
+    st->n_accept = 0;
+    st->min_margin_bits = 0x7ff0000000000000ull;  // +inf
+    st->max_defect_bits = 0;
+  }
+  if (P.W < P.T) {
+    const Real* x0 = static_cast<const Real*>(P.x0);
+    const int64_t n = P.T * P.Dp;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const Real v = x0[i % P.Dp];
+      static_cast<Real*>(P.S[0])[i] = v;
+      static_cast<Real*>(P.S[1])[i] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Finalize: verify the returned trajectory column by column (exact MALA step
+// from S_{t-1} in FP64 log-acceptance), emit accept flags, margins, the
+// recursion defect and logp(S_t) (_trajectory_logps, interface.jl:517-524),
+// and copy the kept columns out.
+// ---------------------------------------------------------------------------
+template <typename Real, int TK, int QPL>
+__global__ void __launch_bounds__(kThreads)
+    deer_finalize_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st) {
+  __shared__ DevParams P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  load_params(Pg, P);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  Smem<Real> sm = carve<Real>(smem_raw, P, 1, TK == kDenseGauss);
+  __syncthreads();
+  const int cur = st->cur;
+  const Real* S = static_cast<const Real*>(P.S[cur]);
+  const Real* x0 = static_cast<const Real*>(P.x0);
+  const TapeKey key(P.seed, P.block);
+  unsigned long long nacc = 0;
+  double min_margin = __longlong_as_double(0x7ff0000000000000ll), max_def = 0.0;
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * kWarps + warp; t < P.T;
+       t += static_cast<int64_t>(gridDim.x) * kWarps) {
+    const Real* xcol = t == 0 ? x0 : S + (t - 1) * Dp;
+    const Real* scol = S + t * Dp;
+    Col<Real, QPL> col;
+    column_forward<Real, TK, QPL>(P, sm, key, xcol, static_cast<int>(t), col);
+    const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+    const bool acc = logu < col.la;
+    double def = 0.0, lp = 0.0;
+    double* vd = TK == kDenseGauss ? sm.Vd + warp * Dp : nullptr;
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        Real s4[4];
+        load4(scol + 4 * j, s4);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          if (4 * j + e >= D) continue;
+          const Real f = acc ? col.y[q][e] : col.x[q][e];
+          def = max(def, static_cast<double>(fabs(s4[e] - f)));
+          const double sd = static_cast<double>(s4[e]) - P.mean_d[4 * j + e];
+          if constexpr (TK == kDiagGauss) lp += -0.5 * P.prec_d[4 * j + e] * sd * sd;
+          else vd[4 * j + e] = sd;
+          if (t < P.ncols_out) {
+            static_cast<Real*>(P.S_out)[t * D + 4 * j + e] = s4[e];
+            if (t == P.ncols_out - 1) static_cast<Real*>(P.x_next)[4 * j + e] = s4[e];
+          }
+        }
+      }
+    }
+    if constexpr (TK == kDenseGauss) {
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < QPL; ++q) {
+        const int j = lane + 32 * q;
+        if (4 * j < D) {
+          double o[4];
+          matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (4 * j + e < D) lp += -0.5 * vd[4 * j + e] * o[e];
+        }
+      }
+      __syncwarp();
+    }
+    lp = warp_sum(lp);
+    def = warp_max(def);
+    if (lane == 0) {
+      if (t < P.ncols_out) {
+        if (P.logp_out) static_cast<Real*>(P.logp_out)[t] = static_cast<Real>(lp);
+        if (P.accept_out) P.accept_out[t] = acc ? 1 : 0;
+      }
+      nacc += acc ? 1 : 0;
+      min_margin = min(min_margin, fabs(col.la - logu));
+      max_def = max(max_def, def);
+    }
+  }
+  if (lane == 0) {
+    if (nacc) atomicAdd(&st->n_accept, nacc);
+    atomicMin(&st->min_margin_bits, dbits(min_margin));
+    if (max_def > 0) atomicMax(&st->max_defect_bits, dbits(max_def));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Unfused evaluation for the plain path: A and B for every column written to
+// HBM (the shape of deer_update!'s batched branch, DEER.jl:398-419).
+// ---------------------------------------------------------------------------
+template <typename Real, int TK, int JAC, int QPL>
+__global__ void __launch_bounds__(kThreads)
+    deer_eval_kernel(const DevParams* __restrict__ Pg, const Real* __restrict__ Sold, int iter,
+                     int from_x0, Real* __restrict__ A, Real* __restrict__ B) {
+  __shared__ DevParams P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  load_params(Pg, P);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  Smem<Real> sm = carve<Real>(smem_raw, P, 1, TK == kDenseGauss);
+  __syncthreads();
+  const Real* x0 = static_cast<const Real*>(P.x0);
+  const TapeKey key(P.seed, P.block);
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * kWarps + warp; t < P.T;
+       t += static_cast<int64_t>(gridDim.x) * kWarps) {
+    const Real* xcol = (t == 0 || from_x0) ? x0 : Sold + (t - 1) * Dp;
+    Col<Real, QPL> col;
+    column_forward<Real, TK, QPL>(P, sm, key, xcol, static_cast<int>(t), col);
+    const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+    const bool acc = logu < col.la;
+    const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
+    const Real gp = static_cast<Real>(gd * (1.0 - gd));
+    Real Aq[QPL][4];
+    column_jacobian<Real, TK, JAC, QPL>(P, sm, key, static_cast<int>(t), iter, acc, gp, col, Aq);
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        Real a4[4], b4[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const Real f = acc ? col.y[q][e] : col.x[q][e];
+          a4[e] = (4 * j + e < D) ? Aq[q][e] : Real(0);
+          b4[e] = (4 * j + e < D) ? f - Aq[q][e] * col.x[q][e] : Real(0);
+        }
+        store4(A + t * Dp + 4 * j, a4);
+        store4(B + t * Dp + 4 * j, b4);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side dispatch
+// ---------------------------------------------------------------------------
+template <typename Real, int TK, int JAC, int QPL>
+static SweepKernels pick3() {
+  SweepKernels k;
+  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, TK, JAC, QPL>);
+  k.finalize = reinterpret_cast<const void*>(&deer_finalize_kernel<Real, TK, QPL>);
+  k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
+  k.eval = reinterpret_cast<const void*>(&deer_eval_kernel<Real, TK, JAC, QPL>);
+  return k;
+}
+
+template <typename Real, int TK, int JAC>
+static SweepKernels pick2(int qpl) {
+  switch (qpl) {
+    case 1: return pick3<Real, TK, JAC, 1>();
+    case 2: return pick3<Real, TK, JAC, 2>();
+    default: return pick3<Real, TK, JAC, 4>();
+  }
+}
+
+template <typename Real>
+static SweepKernels pick1(int tk, int jac, int qpl) {
+  if (tk == kDiagGauss)
+    return jac == kJacStoch ? pick2<Real, kDiagGauss, kJacStoch>(qpl)
+                            : pick2<Real, kDiagGauss, kJacDiag>(qpl);
+  return jac == kJacStoch ? pick2<Real, kDenseGauss, kJacStoch>(qpl)
+                          : pick2<Real, kDenseGauss, kJacDiag>(qpl);
+}
+
+SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D) {
+  const int qpl = D <= 128 ? 1 : (D <= 256 ? 2 : 4);
+  SweepKernels k = f64 ? pick1<double>(tk, jac, qpl) : pick1<float>(tk, jac, qpl);
+  k.qpl = qpl;
+  return k;
+}
+
+SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense) {
+  return f64 ? plan_sweep_smem<double>(Dp, TT, dense) : plan_sweep_smem<float>(Dp, TT, dense);
+}
+
+}  // namespace pmcmc

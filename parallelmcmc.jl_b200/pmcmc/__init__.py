@@ -1,0 +1,22 @@
+"""pmcmc -- B200 DEER hot path of ParallelMCMC.jl behind the reference's sampler API.
+
+The numerics run in libpmcmc_deer.so (hand-written sm_100a CUDA); this package
+is the host-side mirror of the reference interface for that path.
+"""
+from types import SimpleNamespace
+
+from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupported,
+                   default_handle, load)
+from .core import (Chain, DensityModel, ParallelMALASampler, ParallelMALAState,
+                   ParallelMALATransition, sample, solve, solve_affine_scan_diag, step, tape)
+
+# Module-style aliases matching ParallelMCMC.DEER / ParallelMCMC.DEERScan.
+DEER = SimpleNamespace(solve=solve, solve_affine_scan_diag=solve_affine_scan_diag)
+DEERScan = SimpleNamespace(solve_affine_scan_diag=solve_affine_scan_diag)
+
+__all__ = [
+    "ArgumentError", "DimensionMismatch", "DeviceError", "Unsupported", "Handle",
+    "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
+    "ParallelMALAState", "ParallelMALATransition", "sample", "solve", "step", "tape",
+    "solve_affine_scan_diag", "DEER", "DEERScan",
+]

@@ -1,0 +1,175 @@
+"""ctypes binding of libpmcmc_deer.so (the C ABI declared in include/pmcmc_deer.h).
+
+The product path has no CPU fallback: if the library or a CUDA device is
+missing, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libpmcmc_deer.so")
+
+OK, ERR_ARGUMENT, ERR_DIMENSION, ERR_CUDA, ERR_NONFINITE, ERR_TIMEOUT, ERR_UNSUPPORTED, \
+    ERR_NOMEM = range(8)
+JAC = {"stoch_diag": 0, "diag": 1, "full": 2}
+F32, F64 = 0, 1
+MEM_HOST, MEM_DEVICE = 0, 1
+EXEC = {"fused": 0, "plain": 1}
+
+# Exported symbols (kept in step with include/pmcmc_deer.h; tests check both).
+SYMBOLS = [
+    "pmcmc_abi_version", "pmcmc_create", "pmcmc_destroy", "pmcmc_last_error",
+    "pmcmc_target_diag_gauss", "pmcmc_target_dense_gauss", "pmcmc_target_logistic",
+    "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
+    "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
+]
+
+
+class ArgumentError(ValueError):
+    """Counterpart of Julia's ArgumentError (invalid sampler/solver arguments)."""
+
+
+class DimensionMismatch(ValueError):
+    """Counterpart of Julia's DimensionMismatch (inconsistent shapes)."""
+
+
+class DeviceError(RuntimeError):
+    """CUDA failure, bounded-wait timeout or non-finite trajectory."""
+
+
+class Unsupported(NotImplementedError):
+    """A valid request that this build does not implement."""
+
+
+class DeerParams(C.Structure):
+    _fields_ = [
+        ("epsilon", C.c_double), ("T", C.c_int64), ("maxiter", C.c_int32),
+        ("tol_abs", C.c_double), ("tol_rel", C.c_double), ("jacobian", C.c_int32),
+        ("damping", C.c_double), ("probes", C.c_int32), ("window", C.c_int64),
+        ("dtype", C.c_int32), ("exec", C.c_int32),
+    ]
+
+
+class Profile(C.Structure):
+    _fields_ = [("sweep_launches", C.c_int64), ("sweep_ms", C.c_double),
+                ("finalize_launches", C.c_int64), ("finalize_ms", C.c_double)]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("iters", C.c_int32), ("converged", C.c_int32), ("metric", C.c_double),
+        ("n_accept", C.c_int64), ("min_margin", C.c_double), ("max_defect", C.c_double),
+        ("status", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_vp = C.c_void_p
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str = LIB_PATH):
+    """Load the library and declare signatures (no device work)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"{path} is missing: build it with `python parallelmcmc.jl_b200/build.py`")
+        L = C.CDLL(path)
+        L.pmcmc_abi_version.restype = C.c_int
+        L.pmcmc_create.argtypes = [C.c_int, _vp, C.POINTER(_vp)]
+        L.pmcmc_destroy.argtypes = [_vp]
+        L.pmcmc_last_error.restype = C.c_char_p
+        L.pmcmc_last_error.argtypes = [_vp]
+        for fn in ("pmcmc_target_diag_gauss", "pmcmc_target_dense_gauss"):
+            getattr(L, fn).argtypes = [_vp, C.c_int64, _vp, _vp, C.POINTER(_vp)]
+        L.pmcmc_target_logistic.argtypes = [_vp, C.c_int64, C.c_int64, _vp, _vp, C.c_double,
+                                            C.POINTER(_vp)]
+        L.pmcmc_target_destroy.argtypes = [_vp]
+        L.pmcmc_tape.argtypes = [_vp, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64, _vp, _vp,
+                                 C.c_int32]
+        L.pmcmc_deer_solve.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
+                                       C.c_uint64, _vp, _vp, _vp, C.c_int32, C.POINTER(Info)]
+        L.pmcmc_sample.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64, C.c_int64,
+                                   _vp, _vp, _vp, C.c_int32, C.POINTER(Info)]
+        L.pmcmc_affine_scan_diag.argtypes = [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _vp, _vp,
+                                             _vp, C.c_int32]
+        L.pmcmc_set_profiling.argtypes = [_vp, C.c_int32]
+        L.pmcmc_get_profile.argtypes = [_vp, C.POINTER(Profile), C.c_int32]
+        for fn in SYMBOLS:
+            if fn not in ("pmcmc_last_error", "pmcmc_abi_version"):
+                getattr(L, fn).restype = C.c_int
+        _lib = L
+        return L
+
+
+def check(rc: int, handle=None, what: str = ""):
+    if rc == OK:
+        return
+    msg = ""
+    if handle is not None:
+        m = load().pmcmc_last_error(handle)
+        msg = m.decode() if m else ""
+    text = f"{what}: {msg}" if what else msg
+    if rc == ERR_ARGUMENT:
+        raise ArgumentError(text)
+    if rc == ERR_DIMENSION:
+        raise DimensionMismatch(text)
+    if rc == ERR_UNSUPPORTED:
+        raise Unsupported(text)
+    raise DeviceError(f"status {rc}: {text}")
+
+
+class Handle:
+    """One device context: stream, workspace and cached CUDA graph
+    (the DEERWorkspace of DEER.jl:47-90, owned on the device)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        L = load()
+        h = _vp()
+        rc = L.pmcmc_create(int(device), _vp(stream) if stream else None, C.byref(h))
+        if rc != OK:
+            raise DeviceError(f"pmcmc_create(device={device}) failed with status {rc} "
+                              "(no usable CUDA device?)")
+        self.ptr = h
+        self.device = int(device)
+
+    def set_profiling(self, on: bool):
+        check(load().pmcmc_set_profiling(self.ptr, int(bool(on))), self.ptr, "set_profiling")
+
+    def profile(self, reset: bool = True) -> dict:
+        p = Profile()
+        check(load().pmcmc_get_profile(self.ptr, C.byref(p), int(reset)), self.ptr, "profile")
+        return {k: getattr(p, k) for k, _ in p._fields_}
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            load().pmcmc_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_handles: dict[int, Handle] = {}
+
+
+def default_handle(device: int = 0) -> Handle:
+    with _lock:
+        h = _handles.get(device)
+    if h is None:
+        h = Handle(device)
+        with _lock:
+            _handles[device] = h
+    return h

@@ -1,0 +1,327 @@
+"""GPU parity of the C-ABI DEER path against the FP64 CPU oracle on the same tape.
+
+Bars (tolerances are written in each test):
+  * tape and probes: bit-exact;
+  * accept/reject sequences: bit-exact;
+  * positions: the reference's per-column isapprox convention
+    |a - b| <= max(atol, rtol * max(|a|, |b|)) at the reference's own
+    tolerances (test-Deer-vs-MALA.jl:106, 202; test-DEERScan.jl:134), and a
+    1e-5 relative trace error for FP32 state against the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import pmcmc
+from pmcmc import configs
+
+pytestmark = pytest.mark.gpu
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_v1.npz"))
+
+
+@pytest.fixture(scope="module")
+def h():
+    return pmcmc.Handle(0)
+
+
+def trace_err(S, R):
+    """max_t |S_t - R_t|_2 / max(|R_t|_2, 1e-30)."""
+    S = np.asarray(S, np.float64)
+    R = np.asarray(R, np.float64)
+    num = np.linalg.norm(S - R, axis=0)
+    den = np.maximum(np.linalg.norm(R, axis=0), 1e-30)
+    return float(np.max(num / den))
+
+
+def columnwise_close(S, R, rtol, atol):
+    for t in range(R.shape[1]):
+        a, b = np.asarray(S[:, t], np.float64), R[:, t]
+        if np.linalg.norm(a - b) > max(atol, rtol * max(np.linalg.norm(a), np.linalg.norm(b))):
+            return False, t
+    return True, -1
+
+
+# --------------------------------------------------------------------------- tape
+@pytest.mark.parametrize("D,T,seed,block", [(5, 8, 0, 0), (2, 16, 7, 3), (13, 4, 2**40 + 5, 9),
+                                            (100, 333, 1, 2), (257, 5, 11, 0)])
+def test_tape_bit_exact(h, D, T, seed, block):
+    Xi, u = pmcmc.tape(D, T, seed, block, handle=h)
+    Xo, uo = O.tape(seed, block, D, T)
+    assert np.array_equal(np.asarray(Xi), np.asarray(Xo))
+    assert np.array_equal(u, uo)
+    if (seed, block, D, T) == (0, 0, 5, 8):
+        assert np.array_equal(np.asarray(Xi), G["tape_0_0_5_8_Xi"])
+
+
+# --------------------------------------------------------------------------- scan
+def _affine(rng, D, T, dt):
+    A = (0.2 * (rng.random((D, T)) - 0.5)).astype(dt)
+    return A, rng.standard_normal((D, T)).astype(dt), rng.standard_normal(D).astype(dt)
+
+
+@pytest.mark.parametrize("D,T", [(1, 1), (1, 17), (4, 16), (8, 31), (16, 64), (6, 40),
+                                 (3, 100_000), (300, 700), (128, 1024)])
+def test_scan_fp32_matches_sequential(h, D, T):
+    # test-DEERScan.jl:114-172 (FP32, 1e-5)
+    A, B, s0 = _affine(np.random.default_rng(D * 7 + T), D, T, np.float32)
+    S = pmcmc.solve_affine_scan_diag(A, B, s0, handle=h)
+    R = O.scan_seq(A, B, s0)
+    np.testing.assert_allclose(S, R, rtol=1e-5, atol=1e-5)
+    assert O.scan_residual(S, A, B, s0) <= 1e-5
+
+
+@pytest.mark.parametrize("D,T", [(1, 2), (5, 17), (8, 64), (33, 5000)])
+def test_scan_fp64_matches_sequential(h, D, T):
+    # test-DEERScan.jl:37-55 (FP64, 1e-12)
+    A, B, s0 = _affine(np.random.default_rng(T), D, T, np.float64)
+    np.testing.assert_allclose(pmcmc.solve_affine_scan_diag(A, B, s0, handle=h),
+                               O.scan_seq(A, B, s0), rtol=1e-12, atol=1e-12)
+
+
+def test_scan_edge_cases(h):
+    # test-DEERScan.jl:174-223
+    rng = np.random.default_rng(4)
+    A = (rng.random((5, 20)) * 0.2).astype(np.float32)
+    B = np.zeros((5, 20), np.float32)
+    s0 = rng.standard_normal(5).astype(np.float32)
+    np.testing.assert_allclose(pmcmc.solve_affine_scan_diag(A, B, s0, handle=h),
+                               O.scan_seq(A, B, s0), rtol=1e-6, atol=1e-6)
+    A = np.zeros((7, 25), np.float32)
+    B = rng.standard_normal((7, 25)).astype(np.float32)
+    S = pmcmc.solve_affine_scan_diag(A, B, rng.standard_normal(7).astype(np.float32), handle=h)
+    np.testing.assert_allclose(S, B, rtol=1e-6, atol=1e-6)
+    A = (rng.standard_normal((9, 1)) * 0.1).astype(np.float32)
+    B = rng.standard_normal((9, 1)).astype(np.float32)
+    s0 = rng.standard_normal(9).astype(np.float32)
+    S = pmcmc.solve_affine_scan_diag(A, B, s0, handle=h)
+    assert S.shape == (9, 1) and S.dtype == np.float32
+    np.testing.assert_allclose(S, O.scan_seq(A, B, s0), rtol=1e-6, atol=1e-6)
+    S0 = pmcmc.solve_affine_scan_diag(np.zeros((4, 0)), np.zeros((4, 0)), np.zeros(4), handle=h)
+    assert S0.shape == (4, 0)
+
+
+def test_scan_shape_errors(h):
+    A = np.ones((3, 5))
+    with pytest.raises(pmcmc.DimensionMismatch):
+        pmcmc.solve_affine_scan_diag(A, np.ones((3, 4)), np.ones(3), handle=h)
+    with pytest.raises(pmcmc.DimensionMismatch):
+        pmcmc.solve_affine_scan_diag(A, A, np.ones(4), handle=h)
+
+
+def test_scan_device_tensors(h):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(5)
+    A, B, s0 = _affine(rng, 8, 4096, np.float32)
+    S = pmcmc.solve_affine_scan_diag(torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda(),
+                                     torch.from_numpy(s0).cuda(), handle=h)
+    assert S.is_cuda and S.dtype == torch.float32
+    np.testing.assert_allclose(S.cpu().numpy(), O.scan_seq(A, B, s0), rtol=1e-5, atol=1e-5)
+
+
+# --------------------------------------------------------------------------- DEER
+def _oracle_target(model):
+    tg = model.target
+    if tg["kind"] == "diag_gauss":
+        return O.Target.diag_gauss(tg["prec"], tg["mean"])
+    return O.Target.dense_gauss(tg["prec"], tg["mean"])
+
+
+def _run(h, model, sampler, x0, seed, block):
+    return pmcmc.solve(model, sampler, x0, seed=seed, block=block, handle=h, return_logp=True)
+
+
+def test_quickstart_block_matches_oracle_deer_and_sequential(h):
+    model, sampler, x0, meta = configs.quickstart_2d()
+    S, info, lp, acc = _run(h, model, sampler, x0, 0, 0)
+    Xi, u = O.tape(0, 0, 2, 64)
+    tg = _oracle_target(model)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, 0.1, x0, Xi, u)
+    S_cpu, icpu = O.deer_solve(tg, 0.1, x0, Xi, u, 0, 0, tol_abs=1e-6, tol_rel=1e-5)
+    assert info["converged"] and icpu["converged"]
+    assert info["iters"] == icpu["iters"] == G["cfg1_deer_iters"][0]
+    np.testing.assert_allclose(S, S_cpu, rtol=1e-10, atol=1e-12)  # same algorithm, FP64
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) < 1e-4
+    lp_ref = np.array([O.logp(tg, S[:, t]) for t in range(64)])
+    np.testing.assert_allclose(lp, lp_ref, rtol=1e-12, atol=1e-12)
+
+
+def test_diag_jacobian_recovers_sequential(h):
+    # test-Deer-vs-MALA.jl:71-108
+    D, T = 3, 32
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(D))
+    sampler = pmcmc.ParallelMALASampler(0.05, T=T, jacobian="diag", damping=0.5, tol_abs=1e-10,
+                                        tol_rel=1e-8, maxiter=200)
+    x0 = np.random.default_rng(1).standard_normal(D)
+    S, info, _, acc = _run(h, model, sampler, x0, 12345, 1)
+    Xi, u = O.tape(12345, 1, D, T)
+    S_seq, acc_seq, _ = O.mala_sequential(O.Target.diag_gauss(np.ones(D)), 0.05, x0, Xi, u)
+    assert info["converged"]
+    ok, t = columnwise_close(S, S_seq, rtol=1e-6, atol=1e-8)
+    assert ok, f"column {t}"
+    assert np.array_equal(acc, acc_seq)
+
+
+def test_stoch_diag_two_probes_with_rejections(h):
+    # test-Deer-vs-MALA.jl:161-215
+    D, T, eps = 3, 32, 0.15
+    tg = O.Target.diag_gauss(np.ones(D))
+    for blk in range(20):
+        Xi, u = O.tape(777, blk, D, T)
+        x0 = np.random.default_rng(blk).standard_normal(D)
+        S_seq, acc_seq, _ = O.mala_sequential(tg, eps, x0, Xi, u)
+        if (~acc_seq).sum() > 0:
+            break
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(D))
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", probes=2, damping=0.5,
+                                        tol_abs=1e-9, tol_rel=1e-7, maxiter=400)
+    S, info, _, acc = _run(h, model, sampler, x0, 777, blk)
+    assert info["converged"] and (~acc).sum() > 0
+    ok, t = columnwise_close(S, S_seq, rtol=1e-5, atol=1e-7)
+    assert ok, f"column {t}"
+    assert np.array_equal(acc, acc_seq)
+
+
+def test_fp32_diag_gauss_trace_error(h):
+    rng = np.random.default_rng(21)
+    D, T = 100, 2048
+    lam = 10 ** rng.uniform(-1, 1, D)
+    x0 = rng.standard_normal(D).astype(np.float32)
+    model = pmcmc.DensityModel.diag_gaussian(lam)
+    for jac in ("diag", "stoch_diag"):
+        sampler = pmcmc.ParallelMALASampler(0.05, T=T, jacobian=jac, dtype=np.float32,
+                                            tol_abs=1e-7, tol_rel=1e-6, maxiter=400)
+        S, info, _, acc = _run(h, model, sampler, x0, 5, 0)
+        Xi, u = O.tape(5, 0, D, T)
+        S_seq, acc_seq, _ = O.mala_sequential(O.Target.diag_gauss(lam), 0.05,
+                                              x0.astype(np.float64), Xi, u)
+        assert info["converged"], info
+        assert np.array_equal(acc, acc_seq), np.nonzero(acc != acc_seq)[0][:5]
+        assert 0.1 < acc.mean() < 1.0
+        assert trace_err(S, S_seq) <= 1e-5
+
+
+@pytest.mark.parametrize("jac", ["diag", "stoch_diag"])
+def test_fp32_dense_gauss(h, jac):
+    model, sampler, x0, meta = configs.correlated_gauss_d64(T=512, jacobian=jac)
+    sampler.tol_abs, sampler.tol_rel, sampler.maxiter = 1e-7, 1e-6, 500
+    S, info, lp, acc = _run(h, model, sampler, x0, 3, 0)
+    tg = _oracle_target(model)
+    Xi, u = O.tape(3, 0, 64, 512)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, 0.05, x0.astype(np.float64), Xi, u)
+    assert info["converged"], info
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= 1e-5
+    lp_ref = np.array([O.logp(tg, np.asarray(S[:, t], np.float64)) for t in range(0, 512, 37)])
+    np.testing.assert_allclose(lp[::37], lp_ref, rtol=1e-5, atol=1e-4)
+
+
+def test_window_reaches_same_fixed_point(h):
+    rng = np.random.default_rng(22)
+    D, T = 10, 600
+    lam = 10 ** rng.uniform(-1, 1, D)
+    x0 = rng.standard_normal(D)
+    model = pmcmc.DensityModel.diag_gaussian(lam)
+    base = dict(T=T, jacobian="diag", tol_abs=1e-10, tol_rel=1e-9, maxiter=2000, damping=0.5)
+    S_full, i_full = pmcmc.solve(model, pmcmc.ParallelMALASampler(0.05, **base), x0, seed=9,
+                                 handle=h)
+    S_win, i_win = pmcmc.solve(model, pmcmc.ParallelMALASampler(0.05, window=64, **base), x0,
+                               seed=9, handle=h)
+    Xi, u = O.tape(9, 0, D, T)
+    S_seq, _, _ = O.mala_sequential(O.Target.diag_gauss(lam), 0.05, x0, Xi, u)
+    assert i_full["converged"] and i_win["converged"]
+    assert trace_err(S_full, S_seq) < 1e-7 and trace_err(S_win, S_seq) < 1e-7
+
+
+def test_plain_and_fused_agree(h):
+    rng = np.random.default_rng(23)
+    D, T = 40, 3000
+    lam = 10 ** rng.uniform(-1, 1, D)
+    x0 = rng.standard_normal(D).astype(np.float32)
+    model = pmcmc.DensityModel.diag_gaussian(lam)
+    kw = dict(T=T, jacobian="stoch_diag", dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6,
+              maxiter=500)
+    S_f, i_f, _, a_f = _run(h, model, pmcmc.ParallelMALASampler(0.05, **kw), x0, 4, 0)
+    S_p, i_p, _, a_p = _run(h, model, pmcmc.ParallelMALASampler(0.05, exec="plain", **kw), x0, 4,
+                            0)
+    assert i_f["converged"] and i_p["converged"]
+    assert np.array_equal(a_f, a_p)
+    assert trace_err(S_f, S_p) <= 1e-5
+    assert abs(i_f["iters"] - i_p["iters"]) <= 2
+
+
+def test_eager_loop_matches_graph(monkeypatch):
+    monkeypatch.setenv("PMCMC_EAGER", "1")
+    he = pmcmc.Handle(0)
+    monkeypatch.delenv("PMCMC_EAGER")
+    hg = pmcmc.Handle(0)
+    model, sampler, x0, meta = configs.quickstart_2d()
+    Se, ie = pmcmc.solve(model, sampler, x0, seed=3, block=1, handle=he)
+    Sg, ig = pmcmc.solve(model, sampler, x0, seed=3, block=1, handle=hg)
+    assert ie["iters"] == ig["iters"]
+    np.testing.assert_array_equal(Se, Sg)
+
+
+def test_sample_quickstart_matches_fixture(h):
+    # README quick start: 500 samples = 7 full blocks + 52 columns of the 8th
+    model, sampler, x0, meta = configs.quickstart_2d()
+    ch = pmcmc.sample(model, sampler, 500, seed=0, initial_params=x0, handle=h)
+    assert ch.values.shape == (500, 2)
+    assert np.array_equal(ch.accepted, G["cfg1_seq_accept"])
+    assert trace_err(ch.values.T, G["cfg1_seq_values"]) < 1e-4
+    assert ch.info["converged"] == 1
+    assert ch.info["iters"] == int(np.sum(G["cfg1_deer_iters"]))
+
+
+def test_sample_device_tensors_match_host(h):
+    torch = pytest.importorskip("torch")
+    model, sampler, x0, meta = configs.quickstart_2d()
+    a = pmcmc.sample(model, sampler, 300, seed=1, initial_params=x0, handle=h)
+    b = pmcmc.sample(model, sampler, 300, seed=1, initial_params=torch.from_numpy(x0).cuda(),
+                     handle=h)
+    assert b.values.is_cuda
+    np.testing.assert_array_equal(a.values, b.values.cpu().numpy())
+    np.testing.assert_array_equal(a.logp, b.logp.cpu().numpy())
+
+
+def test_step_api_walks_and_resolves(h):
+    # interface.jl:811-869, test-DEER-Interface.jl:127-200
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(3))
+    sampler = pmcmc.ParallelMALASampler(0.05, T=4, jacobian="diag")
+    x0 = np.array([1.0, 2.0, 3.0])
+    x0c = x0.copy()
+    tr, st = pmcmc.step(model, sampler, seed=7, initial_params=x0, handle=h)
+    assert np.array_equal(x0, x0c) and st.t == 1 and st.trajectory.shape == (3, 4)
+    assert abs(tr.logp - model.logdensity(tr.x)) < 1e-12
+    for k in range(2, 5):
+        tr, st = pmcmc.step(model, sampler, st, seed=7, handle=h)
+        assert st.t == k
+    tr, st2 = pmcmc.step(model, sampler, st, seed=7, handle=h)
+    assert st2.t == 1 and st2.block == 1
+
+
+def test_argument_errors_through_c_abi(h):
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(3))
+    for kw in (dict(damping=0.0), dict(damping=1.5), dict(probes=0), dict(maxiter=0),
+               dict(tol_abs=-1.0), dict(tol_rel=-1.0), dict(T=0)):
+        s = pmcmc.ParallelMALASampler(0.1, **kw)
+        with pytest.raises(pmcmc.ArgumentError):
+            pmcmc.solve(model, s, np.zeros(3), handle=h)
+    with pytest.raises(pmcmc.DimensionMismatch):
+        pmcmc.solve(model, pmcmc.ParallelMALASampler(0.1), np.zeros(4), handle=h)
+
+
+def test_full_size_aniso_diag_d100(h):
+    """The D = 100, T = 16384 diagonal-Gaussian workload at full size against the
+    FP64 sequential oracle on the same tape."""
+    model, sampler, x0, meta = configs.aniso_diag_d100()
+    S, info, lp, acc = _run(h, model, sampler, x0, meta["seed"], 0)
+    Xi, u = O.tape(meta["seed"], 0, 100, sampler.T)
+    tg = _oracle_target(model)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, 0.05, x0.astype(np.float64), Xi, u)
+    assert info["converged"]
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= 1e-5
+    assert info["max_defect"] <= 1e-5 * (1 + np.abs(S).max())
