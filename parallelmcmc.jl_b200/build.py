@@ -78,7 +78,8 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
                     print(err, file=sys.stderr)
     if force or todo or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lrt",
-               "-lpthread", "-ldl"]
+               "-lpthread", "-ldl",
+               "-L/usr/local/cuda/lib64", "-lcublas", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

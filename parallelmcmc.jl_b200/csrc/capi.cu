@@ -17,6 +17,7 @@
 #include "../../include/pmcmc_deer.h"
 #include "deer_device.cuh"
 #include "deer_launch.h"
+#include "logistic.h"
 
 using namespace pmcmc;
 
@@ -50,6 +51,7 @@ struct pmcmc_handle {
   bool force_eager = false;
   int tile_override = 0;
   unsigned long long* h_red = nullptr;  // pinned, plain-path metric readback
+  cublasHandle_t cublas = nullptr;
   bool profiling = false;
   pmcmc_profile prof{};
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -63,6 +65,7 @@ struct pmcmc_target {
   double* prec_d = nullptr;
   float* mean_f = nullptr;
   float* prec_f = nullptr;
+  LogisticDev lg;
 };
 
 namespace {
@@ -159,10 +162,12 @@ int choose_tile(pmcmc_handle* h, bool f64, int64_t Dp, int64_t W, bool dense) {
 struct SolveLayout {
   size_t S0, S1, x0a, x0b, flags, agg_a, agg_b, incl, colmax, out_S, out_lp, out_acc;
   size_t pA, pB, al0, be0, al1, be1, red;  // plain path only
+  size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
   size_t total;
 };
 
-SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain) {
+SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain,
+                   int64_t N = 0, int64_t Tc = 0) {
   SolveLayout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -190,6 +195,16 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
     L.al1 = take(es * T * Dp);
     L.be1 = take(es * T * Dp);
     L.red = take(4 * sizeof(unsigned long long));
+  }
+  if (N > 0) {
+    for (int i = 0; i < 5; ++i) L.lg[i] = take(es * T * Dp);
+    L.lpx = take(8 * static_cast<size_t>(T));
+    L.lpy = take(8 * static_cast<size_t>(T));
+    L.acc_col = take(static_cast<size_t>(T));
+    L.la_col = take(8 * static_cast<size_t>(T));
+    L.Bb = take(es * Dp * 2 * Tc);
+    L.Lb = take(es * N * 2 * Tc);
+    L.Gb = take(es * Dp * 2 * Tc);
   }
   L.total = off;
   return L;
@@ -398,6 +413,62 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
   return PMCMC_OK;
 }
 
+// One DEER block for the logistic target: per Newton iteration two GEMM
+// passes (pass 1 at [x_bar | z], pass 2 at [y | w]) feed the fused
+// finish + scan sweep kernel; then a logp pass over the returned trajectory.
+int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
+                 const DevParams& P, const SolveLayout& L, size_t es, size_t smem_sweep,
+                 int fin_grid, int64_t Tc) {
+  unsigned char* ws = h->ws;
+  const bool f64 = es == 8;
+  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  if (smem_sweep > 48 * 1024)
+    CK(cudaFuncSetAttribute(k.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(smem_sweep)));
+  if (!h->cublas) {
+    if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
+      return fail(h, PMCMC_ERR_CUDA, "cublasCreate failed");
+    cublasSetMathMode(h->cublas, CUBLAS_PEDANTIC_MATH);
+  }
+  cublasSetStream(h->cublas, h->stream);
+  void* init_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.init, dim3(1), dim3(256), init_args, 0, h->stream));
+  cudaGraphConditionalHandle none = 0;
+  int zero = 0;
+  void* sweep_args[] = {&h->d_params, &h->d_state, &none, &zero};
+  void *Bb = ws + L.Bb, *Lb = ws + L.Lb, *Gb = ws + L.Gb;
+  for (int it = 0; it < P.maxiter; ++it) {
+    if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpx, 0, P.T,
+                      P.Dp, Bb, Lb, Gb, Tc))
+      return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+    if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpy, 1, P.T,
+                      P.Dp, Bb, Lb, Gb, Tc))
+      return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+    if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
+    CK(cudaLaunchKernel(k.sweep, dim3(P.ntiles), dim3(kThreads), sweep_args, smem_sweep,
+                        h->stream));
+    if (h->profiling) CK(cudaEventRecord(h->ev[1], h->stream));
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->profiling) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+      h->prof.sweep_launches += 1;
+      h->prof.sweep_ms += ms;
+    }
+    if (h->h_state->converged || h->h_state->status) break;
+  }
+  if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpx, 2, P.T,
+                    P.Dp, Bb, Lb, Gb, Tc))
+    return fail(h, PMCMC_ERR_CUDA, "logistic logp pass failed");
+  void* fin_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.finalize, dim3(fin_grid), dim3(kThreads), fin_args, 0, h->stream));
+  return PMCMC_OK;
+}
+
 void fill_info(const DevState& s, pmcmc_info* info) {
   if (!info) return;
   info->iters = s.iter;
@@ -432,8 +503,14 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (mem != PMCMC_MEM_HOST && mem != PMCMC_MEM_DEVICE)
     return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
   if (N < 1) return fail(h, PMCMC_ERR_ARGUMENT, "the number of samples must be >= 1");
-  if (tg->kind == kLogistic)
-    return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target is not built into this library yet");
+  if (tg->kind == kLogistic) {
+    if (p->jacobian != PMCMC_JAC_STOCH_DIAG)
+      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: only :stoch_diag is built");
+    if (p->probes != 1)
+      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: probes must be 1");
+    if (p->window > 0 && p->window < p->T)
+      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: no sliding window");
+  }
   if (p->jacobian == PMCMC_JAC_FULL)
     return fail(h, PMCMC_ERR_UNSUPPORTED, ":full jacobian is not built into this library yet");
   DeviceGuard guard(h->device);
@@ -453,8 +530,11 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (sp_sweep.total > 200 * 1024)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "dimension %lld too large for the fused sweep",
                 (long long)D);
-  const SweepKernels k = gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
-  const SolveLayout L = layout(D, Dp, T, ntiles, es, plain);
+  const bool logistic = tg->kind == kLogistic;
+  const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
+                                  : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
+  const int64_t Tc = logistic ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
+  const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
   unsigned char* ws = h->ws;
@@ -497,6 +577,14 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   P.agg_b = ws + L.agg_b;
   P.incl = ws + L.incl;
   P.colmax = reinterpret_cast<float*>(ws + L.colmax);
+  if (logistic) {
+    for (int i = 0; i < 5; ++i) P.lg[i] = ws + L.lg[i];
+    P.lpx = reinterpret_cast<double*>(ws + L.lpx);
+    P.lpy = reinterpret_cast<double*>(ws + L.lpy);
+    P.acc_col = ws + L.acc_col;
+    P.la_col = reinterpret_cast<double*>(ws + L.la_col);
+    P.tau = tg->lg.tau;
+  }
 
   const int fin_grid = static_cast<int>(std::min<int64_t>((T + kWarps - 1) / kWarps,
                                                           int64_t(h->num_sms) * 8));
@@ -519,8 +607,9 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       P.logp_out = logp_out ? ws + L.out_lp : nullptr;
       P.accept_out = accept_out ? ws + L.out_acc : nullptr;
     }
-    rc = plain ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid)
-               : run_fused(h, k, P, sp_sweep.total, sp_fin.total, fin_grid, init_grid);
+    rc = logistic ? run_logistic(h, tg, k, P, L, es, sp_sweep.total, fin_grid, Tc)
+         : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid)
+                  : run_fused(h, k, P, sp_sweep.total, sp_fin.total, fin_grid, init_grid);
     if (rc) return rc;
     if (mem == PMCMC_MEM_HOST) {
       CK(cudaMemcpyAsync(static_cast<unsigned char*>(S_out) + es * nsteps * D, ws + L.out_S,
@@ -666,6 +755,7 @@ int pmcmc_destroy(pmcmc_handle* h) {
   DeviceGuard guard(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->cublas) cublasDestroy(h->cublas);
   cudaFree(h->ws);
   cudaFree(h->scan_ws);
   cudaFree(h->d_params);
@@ -711,8 +801,44 @@ int pmcmc_target_dense_gauss(pmcmc_handle* h, int64_t D, const double* mean, con
 
 int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X,
                           const double* y, double prior_prec, pmcmc_target** out) {
-  (void)N; (void)D; (void)X; (void)y; (void)prior_prec; (void)out;
-  return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target is not built into this library yet");
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  if (!out || !X || !y) return fail(h, PMCMC_ERR_ARGUMENT, "null argument");
+  if (N < 1 || D < 1) return fail(h, PMCMC_ERR_ARGUMENT, "N and D must be >= 1");
+  if (!(prior_prec > 0)) return fail(h, PMCMC_ERR_ARGUMENT, "prior_prec must be > 0");
+  for (int64_t n = 0; n < N; ++n)
+    if (!(y[n] == 0.0 || y[n] == 1.0)) return fail(h, PMCMC_ERR_ARGUMENT, "labels must be 0 or 1");
+  DeviceGuard guard(h->device);
+  auto* t = new pmcmc_target();
+  t->h = h;
+  t->kind = kLogistic;
+  t->D = D;
+  t->N = N;
+  t->Dp = round4(D);
+  const int64_t Dp = t->Dp;
+  t->lg.N = N;
+  t->lg.D = D;
+  t->lg.Dp = Dp;
+  t->lg.tau = prior_prec;
+  std::vector<double> x64(static_cast<size_t>(N * Dp), 0.0);
+  for (int64_t i = 0; i < D; ++i)
+    for (int64_t n = 0; n < N; ++n) x64[n * Dp + i] = X[i * N + n];
+  std::vector<float> x32(x64.begin(), x64.end());
+  std::vector<float> y32(y, y + N);
+  cudaError_t e = cudaMalloc(&t->lg.X64, 8 * N * Dp);
+  if (e == cudaSuccess) e = cudaMalloc(&t->lg.X32, 4 * N * Dp);
+  if (e == cudaSuccess) e = cudaMalloc(&t->lg.y64, 8 * N);
+  if (e == cudaSuccess) e = cudaMalloc(&t->lg.y32, 4 * N);
+  if (e == cudaSuccess) e = cudaMemcpy(t->lg.X64, x64.data(), 8 * N * Dp, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->lg.X32, x32.data(), 4 * N * Dp, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->lg.y64, y, 8 * N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->lg.y32, y32.data(), 4 * N, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    pmcmc_target_destroy(t);
+    return fail(h, PMCMC_ERR_NOMEM, "logistic target upload failed: %s", cudaGetErrorString(e));
+  }
+  *out = t;
+  return PMCMC_OK;
 }
 
 int pmcmc_target_destroy(pmcmc_target* t) {
@@ -722,6 +848,10 @@ int pmcmc_target_destroy(pmcmc_target* t) {
   cudaFree(t->prec_d);
   cudaFree(t->mean_f);
   cudaFree(t->prec_f);
+  cudaFree(t->lg.X32);
+  cudaFree(t->lg.X64);
+  cudaFree(t->lg.y32);
+  cudaFree(t->lg.y64);
   delete t;
   return PMCMC_OK;
 }

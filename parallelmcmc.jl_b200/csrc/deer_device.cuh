@@ -47,6 +47,15 @@ struct DevParams {
   void* logp_out;
   uint8_t* accept_out;
   void* x_next;  // [D] last kept column (next block's x0)
+  // logistic target: per-column quantities produced by the two GEMM passes
+  // (T x Dp, Real): g_x, y, w = z + eps H(x) z, g_y, H(y) w; likelihood sums
+  // lpx/lpy (T, FP64); the sweep records accept flags and log-alpha per column.
+  void* lg[5];
+  double* lpx;
+  double* lpy;
+  uint8_t* acc_col;
+  double* la_col;
+  double tau;  // prior precision
 };
 
 struct DevState {
@@ -157,36 +166,61 @@ __device__ void tile_scan_inplace(Real* As, Real* Bs, int ncols, int D, int Dp) 
   }
 }
 
-// Decoupled look-back (Merrill & Garland) over per-coordinate affine maps:
-// returns the state entering tile `tile` for coordinate d.  Waits are bounded:
-// after kMaxSpins polls the error flag is set and the call returns.
-template <typename Real>
-__device__ Real lookback_state(int tile, int d, int Dp, uint32_t epoch, const uint32_t* flags,
-                               const Real* agg_a, const Real* agg_b, const Real* incl,
-                               Real s_lo, int* err) {
-  Real a = 1, b = 0;
-  for (int j = tile - 1; j >= 0; --j) {
-    uint32_t f = 0;
-    long long spins = 0;
-    while (true) {
-      f = ld_acquire(flags + j);
-      if ((f >> 2) == (epoch & 0x3fffffffu) && (f & 3u)) break;
-      if (++spins > kMaxSpins) {
-        *err = 1;
-        return Real(0);
+// Decoupled look-back (Merrill & Garland), windowed: warp 0 polls the flags of
+// the 32 nearest predecessors at once and returns the nearest tile j* whose
+// inclusive state is published; every tile in (j*, tile) has published at
+// least its aggregate.  Waits are bounded: on timeout *err = 1 and -1 is
+// returned (the caller records the error and carries on, never hangs).
+__device__ __forceinline__ int lookback_window(int tile, uint32_t epoch, const uint32_t* flags,
+                                               int* err) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t ep = epoch & 0x3fffffffu;
+  for (int hi = tile - 1; hi >= 0; hi -= 32) {
+    const int j = hi - lane;
+    uint32_t st = 0;
+    bool timeout = false;
+    if (j >= 0) {
+      long long spins = 0;
+      while (true) {
+        const uint32_t f = ld_acquire(flags + j);
+        if ((f >> 2) == ep && (f & 3u)) {
+          st = f & 3u;
+          break;
+        }
+        if (++spins > kMaxSpins) {
+          timeout = true;
+          break;
+        }
+        if (spins > 16) __nanosleep(32);
       }
-      __nanosleep(64);
     }
-    if ((f & 3u) == kFlagIncl) {
-      const Real s = __ldcg(incl + static_cast<size_t>(j) * Dp + d);
-      return a * s + b;
+    if (__any_sync(0xffffffffu, timeout)) {
+      *err = 1;
+      return -1;
     }
+    const unsigned incl = __ballot_sync(0xffffffffu, j >= 0 && st == kFlagIncl);
+    if (incl) return hi - (__ffs(incl) - 1);
+  }
+  *err = 1;  // tile 0 always publishes an inclusive state, so this is unreachable
+  return -1;
+}
+
+// State entering `tile` for coordinate d: the aggregates of tiles (jstar, tile)
+// composed onto the inclusive state of jstar.  The loads are independent of
+// the composition chain, so they are issued ahead of it.
+template <typename Real>
+__device__ __forceinline__ Real lookback_compose(int tile, int jstar, int d, int Dp,
+                                                 const Real* agg_a, const Real* agg_b,
+                                                 const Real* incl) {
+  Real a = 1, b = 0;
+#pragma unroll 4
+  for (int j = tile - 1; j > jstar; --j) {
     const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
     const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
     b = a * bj + b;
     a = a * aj;
   }
-  return a * s_lo + b;
+  return a * __ldcg(incl + static_cast<size_t>(jstar) * Dp + d) + b;
 }
 
 }  // namespace pmcmc

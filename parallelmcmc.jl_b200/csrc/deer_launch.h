@@ -21,6 +21,7 @@ struct SweepKernels {
 };
 
 SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D);
+SweepKernels logistic_sweep_kernels(bool f64, int64_t D);
 SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);
 
 // Tape materialisation (tape.cu).

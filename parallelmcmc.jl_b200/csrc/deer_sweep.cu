@@ -225,7 +225,11 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
       const int j = lane + 32 * q;
-      if (4 * j < D) {
+      if (4 * j >= D) {
+        // lanes past the last quad take part in the warp reductions with zeros
+#pragma unroll
+        for (int e = 0; e < 4; ++e) c.gx[q][e] = c.y[q][e] = c.gy[q][e] = Real(0);
+      } else {
         Real lam[4], mu[4];
         double lamd[4], mud[4];
         load4(lamR + 4 * j, lam);
@@ -476,6 +480,90 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
   }
 }
 
+// Logistic target: the gradient / HVP contractions over the N data rows come
+// from the two GEMM passes of this sweep (g_x, y, w, g_y, H(y) w in HBM,
+// likelihood sums in FP64); this evaluates the rest of the batched
+// fwd + JVP (MALA.jl:592-625) for one column and returns A and B.
+template <typename Real, int QPL>
+__device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKey& key,
+                                                const Real* xcol, int t, int iter,
+                                                Real (&A)[QPL][4], Real (&Bv)[QPL][4]) {
+  const int lane = threadIdx.x & 31;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  const Real eps = static_cast<Real>(P.eps), inv2eps = static_cast<Real>(P.inv2eps);
+  const size_t off = static_cast<size_t>(t) * Dp;
+  const Real* gxp = static_cast<const Real*>(P.lg[0]) + off;
+  const Real* yp = static_cast<const Real*>(P.lg[1]) + off;
+  const Real* wp = static_cast<const Real*>(P.lg[2]) + off;
+  const Real* gyp = static_cast<const Real*>(P.lg[3]) + off;
+  const Real* hvp = static_cast<const Real*>(P.lg[4]) + off;
+  Real x[QPL][4], gx[QPL][4], y[QPL][4], gy[QPL][4], w[QPL][4], hvy[QPL][4], z[QPL][4];
+  double la = 0.0;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < D) {
+      load4(xcol + 4 * j, x[q]);
+      load4(gxp + 4 * j, gx[q]);
+      load4(yp + 4 * j, y[q]);
+      load4(gyp + 4 * j, gy[q]);
+      load4(wp + 4 * j, w[q]);
+      load4(hvp + 4 * j, hvy[q]);
+      float xi[4];
+      tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), xi);
+      const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t), 0,
+                               iter);
+      const uint32_t wv = u4_word(pb, (j >> 3) & 3);
+      const int sh = (j & 7) * 4;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        z[q][e] = ((wv >> (sh + e)) & 1u) ? Real(1) : Real(-1);
+        if (4 * j + e < D) {
+          const double xd = static_cast<double>(x[q][e]), yd = static_cast<double>(y[q][e]);
+          const double r1 = P.sqrt2eps * static_cast<double>(xi[e]);
+          const double r2 = (xd - yd) - P.eps * static_cast<double>(gy[q][e]);
+          la += -0.5 * P.tau * (yd * yd - xd * xd) + (r1 * r1 - r2 * r2) * P.inv4eps;
+        } else {
+          z[q][e] = Real(0);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        x[q][e] = gx[q][e] = y[q][e] = gy[q][e] = w[q][e] = hvy[q][e] = z[q][e] = Real(0);
+    }
+  }
+  la = warp_sum(la) + (P.lpy[t] - P.lpx[t]);
+  const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+  const bool acc = logu < la;
+  const double gd = 1.0 / (1.0 + exp(-(la - logu)));
+  const Real gp = static_cast<Real>(gd * (1.0 - gd));
+  Real dla = 0;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const Real r = x[q][e] - y[q][e] - eps * gy[q][e];
+      const Real dr = z[q][e] - w[q][e] - eps * hvy[q][e];
+      dla += gy[q][e] * w[q][e] - gx[q][e] * z[q][e] - inv2eps * r * dr;
+    }
+  dla = warp_sum(dla);
+  const Real dg = gp * dla;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const Real jz = (acc ? w[q][e] : z[q][e]) + (y[q][e] - x[q][e]) * dg;
+      A[q][e] = z[q][e] * jz;
+      const Real f = acc ? y[q][e] : x[q][e];
+      Bv[q][e] = f - A[q][e] * x[q][e];
+    }
+  if (lane == 0) {
+    P.acc_col[t] = acc ? 1 : 0;
+    P.la_col[t] = la - logu;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // The sweep kernel
 // ---------------------------------------------------------------------------
@@ -484,7 +572,7 @@ __global__ void __launch_bounds__(kThreads)
     deer_sweep_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st,
                       cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ DevParams P;
-  __shared__ int s_tile, s_last, s_err, s_nonfinite;
+  __shared__ int s_tile, s_last, s_err, s_nonfinite, s_jstar;
   __shared__ double s_red[2][kWarps];
   extern __shared__ __align__(16) unsigned char smem_raw[];
   load_params(Pg, P);
@@ -551,14 +639,25 @@ __global__ void __launch_bounds__(kThreads)
     const TapeKey key(P.seed, P.block);
     for (int c = warp; c < ncols; c += kWarps) {
       const int t = static_cast<int>(t0 + c);
-      Col<Real, QPL> col;
-      column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col);
-      const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
-      const bool acc = logu < col.la;
-      const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
-      const Real gp = static_cast<Real>(gd * (1.0 - gd));
-      Real A[QPL][4];
-      column_jacobian<Real, TK, JAC, QPL>(P, sm, key, t, iter, acc, gp, col, A);
+      Real A[QPL][4], Bq[QPL][4];
+      if constexpr (TK == kLogistic) {
+        column_logistic<Real, QPL>(P, key, sm.Xs + c * Dp, t, iter, A, Bq);
+      } else {
+        Col<Real, QPL> col;
+        column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col);
+        const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+        const bool acc = logu < col.la;
+        const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
+        const Real gp = static_cast<Real>(gd * (1.0 - gd));
+        column_jacobian<Real, TK, JAC, QPL>(P, sm, key, t, iter, acc, gp, col, A);
+#pragma unroll
+        for (int q = 0; q < QPL; ++q)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const Real f = acc ? col.y[q][e] : col.x[q][e];
+            Bq[q][e] = f - A[q][e] * col.x[q][e];
+          }
+      }
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
         const int j = lane + 32 * q;
@@ -566,9 +665,8 @@ __global__ void __launch_bounds__(kThreads)
           Real a4[4], b4[4];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
-            const Real f = acc ? col.y[q][e] : col.x[q][e];
             a4[e] = (4 * j + e < D) ? A[q][e] : Real(0);
-            b4[e] = (4 * j + e < D) ? f - A[q][e] * col.x[q][e] : Real(0);
+            b4[e] = (4 * j + e < D) ? Bq[q][e] : Real(0);
           }
           store4(sm.As + c * Dp + 4 * j, a4);
           store4(sm.Bs + c * Dp + 4 * j, b4);
@@ -603,14 +701,22 @@ __global__ void __launch_bounds__(kThreads)
       __threadfence();
       __syncthreads();
       if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagAgg);
-      int err = 0;
+      if (warp == 0) {
+        int err = 0;
+        const int js = lookback_window(tile, epoch, P.flags, &err);
+        if (lane == 0) {
+          s_jstar = js;
+          if (err) s_err = 1;
+        }
+      }
+      __syncthreads();
+      const int js = s_jstar;
       for (int d = tid; d < D; d += kThreads) {
-        const Real cin = lookback_state<Real>(tile, d, Dp, epoch, P.flags, agg_a, agg_b, incl,
-                                              sm.Xs[d], &err);
+        const Real cin = js >= 0 ? lookback_compose<Real>(tile, js, d, Dp, agg_a, agg_b, incl)
+                                 : Real(0);
         sm.carry[d] = cin;
         incl[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d] * cin + sm.Bs[last + d];
       }
-      if (err) s_err = 1;
       __threadfence();
       __syncthreads();
       if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagIncl);
@@ -843,10 +949,24 @@ __global__ void __launch_bounds__(kThreads)
       max_def = max(max_def, def);
     }
   }
+  // one atomic per CTA and quantity (same-address atomics from every warp serialise)
+  __shared__ unsigned long long r_acc[kWarps];
+  __shared__ double r_mm[kWarps], r_def[kWarps];
   if (lane == 0) {
-    if (nacc) atomicAdd(&st->n_accept, nacc);
-    atomicMin(&st->min_margin_bits, dbits(min_margin));
-    if (max_def > 0) atomicMax(&st->max_defect_bits, dbits(max_def));
+    r_acc[warp] = nacc;
+    r_mm[warp] = min_margin;
+    r_def[warp] = max_def;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kWarps; ++w) {
+      nacc = r_acc[0] += r_acc[w];
+      min_margin = r_mm[0] = min(r_mm[0], r_mm[w]);
+      max_def = r_def[0] = max(r_def[0], r_def[w]);
+    }
+    if (r_acc[0]) atomicAdd(&st->n_accept, r_acc[0]);
+    atomicMin(&st->min_margin_bits, dbits(r_mm[0]));
+    if (r_def[0] > 0) atomicMax(&st->max_defect_bits, dbits(r_def[0]));
   }
 }
 
@@ -897,6 +1017,61 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Logistic finalize: copy the kept columns out, logp(S_t) from the likelihood
+// sums of the last logp pass (left in lpx) plus the prior, and the accept
+// flags / margins recorded by the last sweep.
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void __launch_bounds__(kThreads)
+    deer_finalize_logistic_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st) {
+  __shared__ DevParams P;
+  load_params(Pg, P);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  const Real* S = static_cast<const Real*>(P.S[st->cur]);
+  unsigned long long nacc = 0;
+  double mm = __longlong_as_double(0x7ff0000000000000ll);
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * kWarps + warp; t < P.T;
+       t += static_cast<int64_t>(gridDim.x) * kWarps) {
+    double q = 0.0;
+    for (int d = lane; d < D; d += 32) {
+      const Real v = S[t * Dp + d];
+      q += static_cast<double>(v) * static_cast<double>(v);
+      if (t < P.ncols_out) {
+        static_cast<Real*>(P.S_out)[t * D + d] = v;
+        if (t == P.ncols_out - 1) static_cast<Real*>(P.x_next)[d] = v;
+      }
+    }
+    q = warp_sum(q);
+    if (lane == 0) {
+      const bool acc = P.acc_col[t] != 0;
+      if (t < P.ncols_out) {
+        if (P.logp_out) static_cast<Real*>(P.logp_out)[t] = static_cast<Real>(P.lpx[t] - 0.5 * P.tau * q);
+        if (P.accept_out) P.accept_out[t] = acc ? 1 : 0;
+      }
+      nacc += acc ? 1 : 0;
+      mm = min(mm, fabs(P.la_col[t]));
+    }
+  }
+  __shared__ unsigned long long r_acc[kWarps];
+  __shared__ double r_mm[kWarps];
+  if (lane == 0) {
+    r_acc[warp] = nacc;
+    r_mm[warp] = mm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kWarps; ++w) {
+      r_acc[0] += r_acc[w];
+      r_mm[0] = min(r_mm[0], r_mm[w]);
+    }
+    if (r_acc[0]) atomicAdd(&st->n_accept, r_acc[0]);
+    atomicMin(&st->min_margin_bits, dbits(r_mm[0]));
+    if (blockIdx.x == 0) atomicMax(&st->max_defect_bits, 0x7ff8000000000000ull);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host-side dispatch
 // ---------------------------------------------------------------------------
 template <typename Real, int TK, int JAC, int QPL>
@@ -925,6 +1100,25 @@ static SweepKernels pick1(int tk, int jac, int qpl) {
                             : pick2<Real, kDiagGauss, kJacDiag>(qpl);
   return jac == kJacStoch ? pick2<Real, kDenseGauss, kJacStoch>(qpl)
                           : pick2<Real, kDenseGauss, kJacDiag>(qpl);
+}
+
+template <typename Real, int QPL>
+static SweepKernels pick_logistic() {
+  SweepKernels k;
+  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL>);
+  k.finalize = reinterpret_cast<const void*>(&deer_finalize_logistic_kernel<Real>);
+  k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
+  k.eval = nullptr;
+  return k;
+}
+
+SweepKernels logistic_sweep_kernels(bool f64, int64_t D) {
+  const int qpl = D <= 128 ? 1 : (D <= 256 ? 2 : 4);
+  SweepKernels k;
+  if (f64) k = qpl == 1 ? pick_logistic<double, 1>() : (qpl == 2 ? pick_logistic<double, 2>() : pick_logistic<double, 4>());
+  else k = qpl == 1 ? pick_logistic<float, 1>() : (qpl == 2 ? pick_logistic<float, 2>() : pick_logistic<float, 4>());
+  k.qpl = qpl;
+  return k;
 }
 
 SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D) {

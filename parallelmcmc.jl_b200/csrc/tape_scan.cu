@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kThreads)
                        const Real* __restrict__ B, const Real* __restrict__ s0,
                        Real* __restrict__ S, ScanScratch scr, uint32_t epoch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_tile, s_err;
+  __shared__ int s_tile, s_err, s_jstar;
   const int tid = threadIdx.x;
   if (tid == 0) {
     s_tile = static_cast<int>(atomicAdd(scr.counter, 1u));
@@ -90,14 +90,22 @@ __global__ void __launch_bounds__(kThreads)
     __threadfence();
     __syncthreads();
     if (tid == 0) st_release(scr.flags + tile, (epoch << 2) | kFlagAgg);
-    int err = 0;
+    if ((tid >> 5) == 0) {
+      int err = 0;
+      const int js = lookback_window(tile, epoch, scr.flags, &err);
+      if (tid == 0) {
+        s_jstar = js;
+        if (err) s_err = 1;
+      }
+    }
+    __syncthreads();
+    const int js = s_jstar;
     for (int d = tid; d < Di; d += kThreads) {
-      const Real c =
-          lookback_state<Real>(tile, d, Di, epoch, scr.flags, agg_a, agg_b, incl, s0[d], &err);
+      const Real c = js >= 0 ? lookback_compose<Real>(tile, js, d, Di, agg_a, agg_b, incl)
+                             : Real(0);
       carry[d] = c;
       incl[static_cast<size_t>(tile) * Di + d] = As[last + d] * c + Bs[last + d];
     }
-    if (err) s_err = 1;
     __threadfence();
     __syncthreads();
     if (tid == 0) st_release(scr.flags + tile, (epoch << 2) | kFlagIncl);

@@ -190,16 +190,26 @@ class ParallelMALASampler:
 
 # --------------------------------------------------------------------------- buffers
 class _Out:
-    """Output buffer on host (NumPy) or device (torch)."""
+    """Output buffer on the device (torch) or on the host: a NumPy array backed by
+    page-locked memory when torch can provide it (the library's device-to-host
+    copies then run at DMA speed), else an ordinary NumPy array."""
 
-    def __init__(self, shape, dtype, like_device: Optional[Any]):
+    def __init__(self, shape, dtype, like_device: Optional[Any], pinned: bool = True):
         self.device = like_device
-        if like_device is not None:
+        tdt = None
+        try:
             import torch
             tdt = {np.float32: torch.float32, np.float64: torch.float64,
                    np.uint8: torch.uint8}[np.dtype(dtype).type]
+        except Exception:
+            torch = None
+        if like_device is not None:
             self.arr = torch.empty(shape, dtype=tdt, device=like_device)
             self.ptr = self.arr.data_ptr()
+        elif pinned and torch is not None and torch.cuda.is_available():
+            self._t = torch.empty(shape, dtype=tdt, pin_memory=True)
+            self.arr = self._t.numpy()
+            self.ptr = self.arr.ctypes.data
         else:
             self.arr = np.empty(shape, dtype=dtype)
             self.ptr = self.arr.ctypes.data

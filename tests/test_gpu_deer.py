@@ -325,3 +325,53 @@ def test_full_size_aniso_diag_d100(h):
     assert np.array_equal(acc, acc_seq)
     assert trace_err(S, S_seq) <= 1e-5
     assert info["max_defect"] <= 1e-5 * (1 + np.abs(S).max())
+
+
+# --------------------------------------------------------------------------- logistic
+def _logistic_problem(N, D, seed):
+    rng = np.random.default_rng(seed)
+    X = (rng.standard_normal((N, D)) / np.sqrt(D)).astype(np.float32).astype(np.float64)
+    th = rng.standard_normal(D)
+    y = (rng.random(N) < 1 / (1 + np.exp(-X @ th))).astype(np.float64)
+    return X, y
+
+
+@pytest.mark.parametrize("dtype,exec_", [(np.float64, "plain"), (np.float32, "plain"),
+                                         (np.float32, "fused")])
+def test_logistic_matches_sequential(h, dtype, exec_):
+    N, D, T, eps = 300, 12, 256, 0.02
+    X, y = _logistic_problem(N, D, 31)
+    model = pmcmc.DensityModel.logistic(X, y)
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", dtype=dtype,
+                                        tol_abs=1e-8, tol_rel=1e-7, maxiter=400, exec=exec_)
+    x0 = np.zeros(D, dtype=dtype)
+    S, info, lp, acc = _run(h, model, sampler, x0, 8, 0)
+    tg = O.Target.logistic(X, y)
+    Xi, u = O.tape(8, 0, D, T)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, eps, np.zeros(D), Xi, u)
+    assert info["converged"], info
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= (1e-9 if dtype == np.float64 else 1e-5)
+    lp_ref = np.array([O.logp(tg, np.asarray(S[:, t], np.float64)) for t in range(0, T, 17)])
+    np.testing.assert_allclose(lp[::17], lp_ref, rtol=1e-5, atol=1e-4)
+
+
+def test_logistic_deer_iterations_match_cpu_deer(h):
+    N, D, T, eps = 200, 8, 128, 0.02
+    X, y = _logistic_problem(N, D, 32)
+    model = pmcmc.DensityModel.logistic(X, y)
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", dtype=np.float64,
+                                        exec="plain")
+    S, info = pmcmc.solve(model, sampler, np.zeros(D), seed=9, handle=h)
+    Xi, u = O.tape(9, 0, D, T)
+    S_cpu, icpu = O.deer_solve(O.Target.logistic(X, y), eps, np.zeros(D), Xi, u, 9, 0)
+    assert info["iters"] == icpu["iters"]
+    np.testing.assert_allclose(S, S_cpu, rtol=1e-9, atol=1e-10)
+
+
+def test_logistic_unsupported_modes(h):
+    X, y = _logistic_problem(50, 4, 33)
+    model = pmcmc.DensityModel.logistic(X, y)
+    with pytest.raises(pmcmc.Unsupported):
+        pmcmc.solve(model, pmcmc.ParallelMALASampler(0.01, T=16, jacobian="diag"), np.zeros(4),
+                    handle=h)
