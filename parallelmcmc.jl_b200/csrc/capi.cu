@@ -23,10 +23,11 @@ using namespace pmcmc;
 
 struct GraphKey {
   const void* sweep = nullptr;
+  bool coop = false;
   int ntiles = 0, fin_grid = 0, init_grid = 0;
   size_t smem_sweep = 0, smem_fin = 0;
   bool operator==(const GraphKey& o) const {
-    return sweep == o.sweep && ntiles == o.ntiles && fin_grid == o.fin_grid &&
+    return sweep == o.sweep && coop == o.coop && ntiles == o.ntiles && fin_grid == o.fin_grid &&
            init_grid == o.init_grid && smem_sweep == o.smem_sweep && smem_fin == o.smem_fin;
   }
 };
@@ -49,6 +50,7 @@ struct pmcmc_handle {
   cudaGraphConditionalHandle cond = 0;
   GraphKey gkey;
   bool force_eager = false;
+  bool no_coop = false;
   int tile_override = 0;
   unsigned long long* h_red = nullptr;  // pinned, plain-path metric readback
   cublasHandle_t cublas = nullptr;
@@ -150,12 +152,53 @@ int validate(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p)
   return PMCMC_OK;
 }
 
-int choose_tile(pmcmc_handle* h, bool f64, int64_t Dp, int64_t W, bool dense) {
-  if (h->tile_override > 0) return h->tile_override;
+struct TilePlan {
+  int TT = 8;
+  bool coop = false;
+};
+
+// Smallest tile (most parallelism) whose every CTA is co-resident -> the
+// cooperative sweep; otherwise the decoupled look-back sweep with a tile that
+// keeps about two CTAs per SM busy.
+TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t Dp, int64_t W,
+                     bool dense) {
+  TilePlan tp;
+  if (h->tile_override > 0) {
+    tp.TT = h->tile_override;
+    tp.coop = false;
+    return tp;
+  }
+  if (!h->no_coop && k.sweep_coop) {
+    for (int TT = 8; TT <= 256; TT <<= 1) {
+      const size_t smem = gauss_sweep_smem(f64, Dp, TT, dense).total;
+      if (smem > 200 * 1024) break;
+      cudaFuncSetAttribute(k.sweep_coop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem));
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.sweep_coop, kThreads, smem) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        break;
+      }
+      if (nb > 0 && (W + TT - 1) / TT <= static_cast<int64_t>(nb) * h->num_sms) {
+        tp.TT = TT;
+        tp.coop = true;
+        return tp;
+      }
+    }
+  }
   int TT = 64;
   while (TT > 8 && gauss_sweep_smem(f64, Dp, TT, dense).total > 100 * 1024) TT >>= 1;
   while (TT > 8 && (W + TT - 1) / TT < 2 * h->num_sms) TT >>= 1;
-  return TT;
+  tp.TT = TT;
+  return tp;
+}
+
+cudaError_t launch_sweep(const void* fn, bool coop, int grid, size_t smem, void** args,
+                         cudaStream_t s) {
+  if (coop)
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, s);
+  return cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, smem, s);
 }
 
 // Workspace carve-up for one solve.
@@ -249,12 +292,17 @@ int build_graph(pmcmc_handle* h, const SweepKernels& k, const GraphKey& key, int
   if (e == cudaSuccess) {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     cudaKernelNodeParams sp{};
-    sp.func = const_cast<void*>(k.sweep);
+    sp.func = const_cast<void*>(key.sweep);
     sp.gridDim = dim3(key.ntiles);
     sp.blockDim = dim3(kThreads);
     sp.sharedMemBytes = static_cast<unsigned>(key.smem_sweep);
     sp.kernelParams = sweep_args;
     e = cudaGraphAddKernelNode(&n_sweep, body, nullptr, 0, &sp);
+    if (e == cudaSuccess && key.coop) {
+      cudaLaunchAttributeValue v{};
+      v.cooperative = 1;
+      e = cudaGraphKernelNodeSetAttribute(n_sweep, cudaLaunchAttributeCooperative, &v);
+    }
   }
   if (e == cudaSuccess) {
     cudaKernelNodeParams fp{};
@@ -277,18 +325,20 @@ int build_graph(pmcmc_handle* h, const SweepKernels& k, const GraphKey& key, int
 
 // One DEER block on the fused path.  Outputs go to the pointers in `P`
 // (already filled by the caller); the state of the solve stays in d_state.
-int run_fused(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t smem_sweep,
-              size_t smem_fin, int fin_grid, int init_grid) {
+int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams& P,
+              size_t smem_sweep, size_t smem_fin, int fin_grid, int init_grid) {
+  const void* sweep_fn = coop ? k.sweep_coop : k.sweep;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 48 * 1024)
-    CK(cudaFuncSetAttribute(k.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(sweep_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem_sweep)));
   if (smem_fin > 48 * 1024)
     CK(cudaFuncSetAttribute(k.finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem_fin)));
   if (!h->force_eager && !h->profiling) {
     GraphKey key;
-    key.sweep = k.sweep;
+    key.sweep = sweep_fn;
+    key.coop = coop;
     key.ntiles = P.ntiles;
     key.fin_grid = fin_grid;
     key.init_grid = init_grid;
@@ -309,8 +359,7 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t
   void* sweep_args[] = {&h->d_params, &h->d_state, &none, &zero};
   for (int it = 0; it < P.maxiter; ++it) {
     if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
-    CK(cudaLaunchKernel(k.sweep, dim3(P.ntiles), dim3(kThreads), sweep_args, smem_sweep,
-                        h->stream));
+    CK(launch_sweep(sweep_fn, coop, P.ntiles, smem_sweep, sweep_args, h->stream));
     if (h->profiling) {
       // one sweep at a time so that only real sweeps are timed
       CK(cudaEventRecord(h->ev[1], h->stream));
@@ -416,14 +465,15 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
 // One DEER block for the logistic target: per Newton iteration two GEMM
 // passes (pass 1 at [x_bar | z], pass 2 at [y | w]) feed the fused
 // finish + scan sweep kernel; then a logp pass over the returned trajectory.
-int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
+int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k, bool coop,
                  const DevParams& P, const SolveLayout& L, size_t es, size_t smem_sweep,
                  int fin_grid, int64_t Tc) {
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 48 * 1024)
-    CK(cudaFuncSetAttribute(k.sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(coop ? k.sweep_coop : k.sweep,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem_sweep)));
   if (!h->cublas) {
     if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
@@ -447,8 +497,8 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
       return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
                   cudaGetErrorString(cudaGetLastError()));
     if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
-    CK(cudaLaunchKernel(k.sweep, dim3(P.ntiles), dim3(kThreads), sweep_args, smem_sweep,
-                        h->stream));
+    CK(launch_sweep(coop ? k.sweep_coop : k.sweep, coop, P.ntiles, smem_sweep, sweep_args,
+                    h->stream));
     if (h->profiling) CK(cudaEventRecord(h->ev[1], h->stream));
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
                        h->stream));
@@ -523,16 +573,17 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   const bool plain = p->exec == PMCMC_EXEC_PLAIN;
   if (plain && W < T)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "the plain path has no sliding window");
-  const int TT = choose_tile(h, f64, Dp, W, dense);
+  const bool logistic = tg->kind == kLogistic;
+  const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
+                                  : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
+  const TilePlan tp = choose_tile(h, k, f64, Dp, W, dense);
+  const int TT = tp.TT;
   const int ntiles = static_cast<int>((W + TT - 1) / TT);
   const SmemPlan sp_sweep = gauss_sweep_smem(f64, Dp, TT, dense);
   const SmemPlan sp_fin = gauss_sweep_smem(f64, Dp, 1, dense);
   if (sp_sweep.total > 200 * 1024)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "dimension %lld too large for the fused sweep",
                 (long long)D);
-  const bool logistic = tg->kind == kLogistic;
-  const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
-                                  : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
   const int64_t Tc = logistic ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc);
   rc = ensure_ws(h, L.total);
@@ -607,9 +658,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       P.logp_out = logp_out ? ws + L.out_lp : nullptr;
       P.accept_out = accept_out ? ws + L.out_acc : nullptr;
     }
-    rc = logistic ? run_logistic(h, tg, k, P, L, es, sp_sweep.total, fin_grid, Tc)
+    rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid, Tc)
          : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid)
-                  : run_fused(h, k, P, sp_sweep.total, sp_fin.total, fin_grid, init_grid);
+                  : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
+                              init_grid);
     if (rc) return rc;
     if (mem == PMCMC_MEM_HOST) {
       CK(cudaMemcpyAsync(static_cast<unsigned char*>(S_out) + es * nsteps * D, ws + L.out_S,
@@ -739,6 +791,8 @@ int pmcmc_create(int device, void* stream, pmcmc_handle** out) {
   cudaMemset(h->d_params, 0, sizeof(DevParams));
   const char* ev = std::getenv("PMCMC_EAGER");
   h->force_eager = ev && ev[0] == '1';
+  const char* cv = std::getenv("PMCMC_NO_COOP");
+  h->no_coop = cv && cv[0] == '1';
   const char* tv = std::getenv("PMCMC_TILE_COLS");
   h->tile_override = tv ? std::atoi(tv) : 0;
   if (cudaDeviceSynchronize() != cudaSuccess) {

@@ -14,6 +14,7 @@ struct SmemPlan {
 
 struct SweepKernels {
   const void* sweep = nullptr;     // (const DevParams*, DevState*, cudaGraphConditionalHandle, int)
+  const void* sweep_coop = nullptr;  // same signature, cooperative launch (all tiles resident)
   const void* finalize = nullptr;  // (const DevParams*, DevState*)
   const void* init = nullptr;      // (const DevParams*, DevState*)
   const void* eval = nullptr;      // (const DevParams*, const Real* Sold, int iter, int from_x0, Real* A, Real* B)

@@ -14,12 +14,15 @@
 // tape (xi, u) and the probes are regenerated in registers, so a sweep reads
 // and writes the trajectory once.  The last CTA to finish evaluates the
 // convergence test and drives the CUDA-graph while-node.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 #include "deer_device.cuh"
 #include "deer_launch.h"
+
+namespace cg = cooperative_groups;
 
 namespace pmcmc {
 
@@ -564,15 +567,65 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
   }
 }
 
+// Cooperative sweep, phase B: for coordinate d, the state entering every tile
+// (exclusive scan of the tile aggregates in tile order, applied to s_lo) by
+// one CTA: each thread composes a run of consecutive tiles, a Kogge-Stone scan
+// over the 256 run aggregates in shared memory, then each run is replayed.
+template <typename Real>
+__device__ void carry_scan_tiles(int ntiles, int d, int Dp, const Real* __restrict__ agg_a,
+                                 const Real* __restrict__ agg_b, Real s_lo,
+                                 Real* __restrict__ carry, Real* sa, Real* sb) {
+  const int tid = threadIdx.x;
+  const int K = (ntiles + kThreads - 1) / kThreads;
+  const int j0 = min(ntiles, tid * K), j1 = min(ntiles, j0 + K);
+  Real a = 1, b = 0;
+  for (int j = j0; j < j1; ++j) {
+    const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
+    const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
+    b = aj * b + bj;
+    a = aj * a;
+  }
+  sa[tid] = a;
+  sb[tid] = b;
+  __syncthreads();
+  for (int off = 1; off < kThreads; off <<= 1) {
+    Real pa = 1, pb = 0;
+    if (tid >= off) {
+      pa = sa[tid - off];
+      pb = sb[tid - off];
+    }
+    __syncthreads();
+    if (tid >= off) {
+      const Real ma = sa[tid], mb = sb[tid];
+      sa[tid] = ma * pa;
+      sb[tid] = ma * pb + mb;
+    }
+    __syncthreads();
+  }
+  Real st = s_lo;
+  if (tid > 0) st = sa[tid - 1] * s_lo + sb[tid - 1];
+  for (int j = j0; j < j1; ++j) {
+    carry[static_cast<size_t>(j) * Dp + d] = st;
+    const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
+    const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
+    st = aj * st + bj;
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // The sweep kernel
 // ---------------------------------------------------------------------------
-template <typename Real, int TK, int JAC, int QPL>
+// COOP = true: launched cooperatively with every tile resident; the cross-tile
+// scan is two grid-wide barriers around a per-coordinate scan of the tile
+// aggregates (no look-back chains).  COOP = false: decoupled look-back.
+template <typename Real, int TK, int JAC, int QPL, bool COOP>
 __global__ void __launch_bounds__(kThreads)
     deer_sweep_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st,
                       cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ DevParams P;
   __shared__ int s_tile, s_last, s_err, s_nonfinite, s_jstar;
+  __shared__ Real s_sa[kThreads], s_sb[kThreads];
   __shared__ double s_red[2][kWarps];
   extern __shared__ __align__(16) unsigned char smem_raw[];
   load_params(Pg, P);
@@ -590,7 +643,8 @@ __global__ void __launch_bounds__(kThreads)
   const int64_t t_lo_prev = *reinterpret_cast<volatile int64_t*>(&st->t_lo_prev);
   const uint32_t epoch = *reinterpret_cast<volatile uint32_t*>(&st->epoch);
   if (tid == 0) {
-    s_tile = static_cast<int>(atomicAdd(&st->tile_counter, 1u));
+    s_tile = COOP ? static_cast<int>(blockIdx.x)
+                  : static_cast<int>(atomicAdd(&st->tile_counter, 1u));
     s_err = 0;
     s_nonfinite = 0;
   }
@@ -679,50 +733,79 @@ __global__ void __launch_bounds__(kThreads)
     tile_scan_inplace<Real>(sm.As, sm.Bs, ncols, D, Dp);
     __syncthreads();
 
-    // ---- phase 3: decoupled look-back for the state entering the tile ----
+    // ---- phase 3: state entering the tile ----
     Real* agg_a = static_cast<Real*>(P.agg_a);
     Real* agg_b = static_cast<Real*>(P.agg_b);
     Real* incl = static_cast<Real*>(P.incl);
     const size_t last = static_cast<size_t>(ncols - 1) * Dp;
-    if (tile == 0) {
-      for (int d = tid; d < D; d += kThreads) {
-        const Real s_lo = sm.Xs[d];
-        sm.carry[d] = s_lo;
-        incl[d] = sm.As[last + d] * s_lo + sm.Bs[last + d];
-      }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) st_release(P.flags, (epoch << 2) | kFlagIncl);
-    } else {
+    if constexpr (COOP) {
       for (int d = tid; d < D; d += kThreads) {
         agg_a[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d];
         agg_b[static_cast<size_t>(tile) * Dp + d] = sm.Bs[last + d];
       }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagAgg);
-      if (warp == 0) {
-        int err = 0;
-        const int js = lookback_window(tile, epoch, P.flags, &err);
-        if (lane == 0) {
-          s_jstar = js;
-          if (err) s_err = 1;
+    } else {
+      if (tile == 0) {
+        for (int d = tid; d < D; d += kThreads) {
+          const Real s_lo = sm.Xs[d];
+          sm.carry[d] = s_lo;
+          incl[d] = sm.As[last + d] * s_lo + sm.Bs[last + d];
         }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(P.flags, (epoch << 2) | kFlagIncl);
+      } else {
+        for (int d = tid; d < D; d += kThreads) {
+          agg_a[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d];
+          agg_b[static_cast<size_t>(tile) * Dp + d] = sm.Bs[last + d];
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagAgg);
+        if (warp == 0) {
+          int err = 0;
+          const int js = lookback_window(tile, epoch, P.flags, &err);
+          if (lane == 0) {
+            s_jstar = js;
+            if (err) s_err = 1;
+          }
+        }
+        __syncthreads();
+        const int js = s_jstar;
+        for (int d = tid; d < D; d += kThreads) {
+          const Real cin = js >= 0 ? lookback_compose<Real>(tile, js, d, Dp, agg_a, agg_b, incl)
+                                   : Real(0);
+          sm.carry[d] = cin;
+          incl[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d] * cin + sm.Bs[last + d];
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagIncl);
       }
       __syncthreads();
-      const int js = s_jstar;
-      for (int d = tid; d < D; d += kThreads) {
-        const Real cin = js >= 0 ? lookback_compose<Real>(tile, js, d, Dp, agg_a, agg_b, incl)
-                                 : Real(0);
-        sm.carry[d] = cin;
-        incl[static_cast<size_t>(tile) * Dp + d] = sm.As[last + d] * cin + sm.Bs[last + d];
-      }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagIncl);
+    }
+  }
+
+  if constexpr (COOP) {
+    // ---- phase B: per-coordinate scan of the tile aggregates (all CTAs) ----
+    cg::grid_group grid = cg::this_grid();
+    grid.sync();
+    const int nact = static_cast<int>((t_hi - t_lo + TT - 1) / TT);
+    const Real* agg_a = static_cast<const Real*>(P.agg_a);
+    const Real* agg_b = static_cast<const Real*>(P.agg_b);
+    Real* incl = static_cast<Real*>(P.incl);
+    for (int d = blockIdx.x; d < D; d += gridDim.x) {
+      const Real s_lo = (from_x0 || t_lo == 0) ? x0[d] : Sold[(t_lo - 1) * Dp + d];
+      carry_scan_tiles<Real>(nact, d, Dp, agg_a, agg_b, s_lo, incl, s_sa, s_sb);
+    }
+    grid.sync();
+    if (ncols > 0) {
+      for (int d = tid; d < D; d += kThreads)
+        sm.carry[d] = __ldcg(incl + static_cast<size_t>(tile) * Dp + d);
     }
     __syncthreads();
+  }
 
+  if (ncols > 0) {
     // ---- phase 4: apply carry, damping, metric, write S_new ----
     const Real dmp = static_cast<Real>(P.damping), omd = static_cast<Real>(1.0 - P.damping);
     const bool undamped = P.damping == 1.0;
@@ -785,8 +868,14 @@ __global__ void __launch_bounds__(kThreads)
     if (s_err) atomicExch(&st->status, static_cast<int>(kStTimeout));
     if (s_nonfinite) atomicCAS(&st->status, 0, static_cast<int>(kStNonfinite));
     __threadfence();
-    const unsigned prev = atomicAdd(&st->done_counter, 1u);
-    s_last = (prev == gridDim.x - 1);
+    if constexpr (!COOP) {
+      const unsigned prev = atomicAdd(&st->done_counter, 1u);
+      s_last = (prev == gridDim.x - 1);
+    }
+  }
+  if constexpr (COOP) {
+    cg::this_grid().sync();
+    if (tid == 0) s_last = blockIdx.x == 0;
   }
   __syncthreads();
   if (!s_last) return;
@@ -1077,7 +1166,8 @@ __global__ void __launch_bounds__(kThreads)
 template <typename Real, int TK, int JAC, int QPL>
 static SweepKernels pick3() {
   SweepKernels k;
-  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, TK, JAC, QPL>);
+  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, TK, JAC, QPL, false>);
+  k.sweep_coop = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, TK, JAC, QPL, true>);
   k.finalize = reinterpret_cast<const void*>(&deer_finalize_kernel<Real, TK, QPL>);
   k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
   k.eval = reinterpret_cast<const void*>(&deer_eval_kernel<Real, TK, JAC, QPL>);
@@ -1105,7 +1195,8 @@ static SweepKernels pick1(int tk, int jac, int qpl) {
 template <typename Real, int QPL>
 static SweepKernels pick_logistic() {
   SweepKernels k;
-  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL>);
+  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL, false>);
+  k.sweep_coop = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL, true>);
   k.finalize = reinterpret_cast<const void*>(&deer_finalize_logistic_kernel<Real>);
   k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
   k.eval = nullptr;

@@ -26,11 +26,14 @@ def cases():
     # probes
     out["probe_3_1_2_1_300_4"] = O.probe(3, 1, 2, 1, 300, 4)
 
-    # config-1 quick start: D=2 standard normal, eps 0.1, T=64, stoch_diag, x0 = 0, 500 samples
+    # config-1 quick start: D=2 standard normal, eps 0.1, T=64, stoch_diag, x0 = 0, 500 samples.
+    # Blocks chain like the reference's block loop (interface.jl:584-599): block b+1
+    # starts from the last kept column of block b's DEER solution.  The sequential
+    # trace of each block starts from the same state.
     D, T, N, eps = 2, 64, 500, 0.1
     tg = O.Target.diag_gauss(np.ones(D))
     x = np.zeros(D)
-    vals, accs, iters = [], [], []
+    vals, seqs, accs, iters = [], [], [], []
     nsteps, b = 0, 0
     while nsteps < N:
         Xi, u = O.tape(0, b, D, T)
@@ -38,14 +41,15 @@ def cases():
         S_deer, info = O.deer_solve(tg, eps, x, Xi, u, 0, b, jacobian="stoch_diag", probes=1,
                                     damping=0.5, tol_abs=1e-6, tol_rel=1e-5, maxiter=200)
         nkeep = min(T, N - nsteps)
-        vals.append(S_seq[:, :nkeep])
+        vals.append(S_deer[:, :nkeep])
+        seqs.append(S_seq[:, :nkeep])
         accs.append(acc[:nkeep])
         iters.append(info["iters"])
-        out[f"cfg1_block{b}_deer"] = S_deer
-        x = S_seq[:, nkeep - 1].copy()
+        x = S_deer[:, nkeep - 1].copy()
         nsteps += nkeep
         b += 1
-    out["cfg1_seq_values"] = np.concatenate(vals, axis=1)
+    out["cfg1_deer_values"] = np.concatenate(vals, axis=1)
+    out["cfg1_seq_values"] = np.concatenate(seqs, axis=1)
     out["cfg1_seq_accept"] = np.concatenate(accs)
     out["cfg1_deer_iters"] = np.asarray(iters)
 

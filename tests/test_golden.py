@@ -20,22 +20,26 @@ def test_config1_fixture():
     D, T, N, eps = 2, 64, 500, 0.1
     tg = O.Target.diag_gauss(np.ones(D))
     x = np.zeros(D)
-    vals = []
+    vals, seqs, iters = [], [], []
     nsteps, b = 0, 0
     while nsteps < N:
         Xi, u = O.tape(0, b, D, T)
         S, acc, _ = O.mala_sequential(tg, eps, x, Xi, u)
+        Sd, info = O.deer_solve(tg, eps, x, Xi, u, 0, b, tol_abs=1e-6, tol_rel=1e-5)
         nkeep = min(T, N - nsteps)
-        vals.append(S[:, :nkeep])
-        x = S[:, nkeep - 1].copy()
+        vals.append(Sd[:, :nkeep])
+        seqs.append(S[:, :nkeep])
+        iters.append(info["iters"])
+        x = Sd[:, nkeep - 1].copy()
         nsteps += nkeep
         b += 1
-    np.testing.assert_allclose(np.concatenate(vals, axis=1), G["cfg1_seq_values"], rtol=1e-13,
+    np.testing.assert_allclose(np.concatenate(vals, axis=1), G["cfg1_deer_values"], rtol=1e-12,
+                               atol=1e-12)
+    np.testing.assert_allclose(np.concatenate(seqs, axis=1), G["cfg1_seq_values"], rtol=1e-13,
                                atol=1e-13)
-    Xi, u = O.tape(0, 0, D, T)
-    S, info = O.deer_solve(tg, eps, np.zeros(D), Xi, u, 0, 0, tol_abs=1e-6, tol_rel=1e-5)
-    np.testing.assert_allclose(S, G["cfg1_block0_deer"], rtol=1e-12, atol=1e-12)
-    assert info["iters"] == G["cfg1_deer_iters"][0]
+    assert list(iters) == list(G["cfg1_deer_iters"])
+    # DEER and the sequential chain agree to the solver tolerance
+    assert np.max(np.abs(G["cfg1_deer_values"] - G["cfg1_seq_values"])) < 1e-3
 
 
 def test_diag_and_dense_fixtures():
