@@ -156,6 +156,26 @@ int pmcmc_sample(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params
 int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T, const void* A,
                            const void* B, const void* s0, void* S, int32_t mem);
 
+/* ---- diagonal affine scan without allocation ----------------------------------
+ * No counterpart in the reference.  For callers that may not call cudaMalloc
+ * once running (a process whose own pool already owns the device memory, such
+ * as a Julia session with CUDA.jl's pool or a serving process with a fixed
+ * memory budget, or a latency-critical loop that cannot take an allocation's
+ * implicit synchronisation): the same scan as pmcmc_affine_scan_diag, with A,
+ * B, s0 and S device pointers on the current device and no handle.  The
+ * look-back scratch is a static device array of PMCMC_NOALLOC_SCRATCH_BYTES
+ * (4 MiB) that every GPU loading the library holds until the process exits;
+ * no cudaMalloc, cudaFree or allocating library routine is called.  A size
+ * whose scratch exceeds the array returns PMCMC_ERR_NOMEM (the scratch needed
+ * is about 3 * sizeof(element) * D * ceil(T / tile) bytes, tile <= 64 columns).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU (other streams or host threads) race and must be
+ * serialised by the caller.  Synchronises `stream` before returning. */
+#define PMCMC_NOALLOC_SCRATCH_BYTES (4u << 20)
+int pmcmc_affine_scan_diag_noalloc(int32_t dtype, int64_t D, int64_t T, const void* A,
+                                   const void* B, const void* s0, void* S, void* stream);
+
 /* ---- profiling ------------------------------------------------------------
  * With profiling on, solves run their Newton loop as individual launches with
  * CUDA events around every sweep and finalize kernel (no graph); the device

@@ -25,6 +25,7 @@ SYMBOLS = [
     "pmcmc_target_diag_gauss", "pmcmc_target_dense_gauss", "pmcmc_target_logistic",
     "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
+    "pmcmc_affine_scan_diag_noalloc",
 ]
 
 
@@ -102,6 +103,8 @@ def load(path: str = LIB_PATH):
                                    _vp, _vp, _vp, C.c_int32, C.POINTER(Info)]
         L.pmcmc_affine_scan_diag.argtypes = [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _vp, _vp,
                                              _vp, C.c_int32]
+        L.pmcmc_affine_scan_diag_noalloc.argtypes = [C.c_int32, C.c_int64, C.c_int64, _vp, _vp,
+                                                     _vp, _vp, _vp]
         L.pmcmc_set_profiling.argtypes = [_vp, C.c_int32]
         L.pmcmc_get_profile.argtypes = [_vp, C.POINTER(Profile), C.c_int32]
         for fn in SYMBOLS:
