@@ -3,6 +3,7 @@
 // Host-side runtime: handle (device, stream, workspace, cached CUDA graph),
 // device targets, argument validation with the reference's error classes, the
 // Newton loop driver and the block loop of the sampler.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -206,11 +207,13 @@ struct SolveLayout {
   size_t S0, S1, x0a, x0b, flags, agg_a, agg_b, incl, colmax, out_S, out_lp, out_acc;
   size_t pA, pB, al0, be0, al1, be1, red;  // plain path only
   size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
+  size_t xi, logu;
+  size_t tcws, Gtc;  // tensor-core logistic path
   size_t total;
 };
 
 SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain,
-                   int64_t N = 0, int64_t Tc = 0) {
+                   int64_t N = 0, int64_t Tc = 0, size_t tc_bytes = 0) {
   SolveLayout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -230,6 +233,8 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
   L.out_S = take(es * T * D);
   L.out_lp = take(es * T);
   L.out_acc = take(static_cast<size_t>(T));
+  L.xi = take(4 * T * Dp);
+  L.logu = take(8 * static_cast<size_t>(T));
   if (plain) {
     L.pA = take(es * T * Dp);
     L.pB = take(es * T * Dp);
@@ -248,6 +253,10 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
     L.Bb = take(es * Dp * 2 * Tc);
     L.Lb = take(es * N * 2 * Tc);
     L.Gb = take(es * Dp * 2 * Tc);
+  }
+  if (tc_bytes) {
+    L.tcws = take(tc_bytes);
+    L.Gtc = take(4 * Dp * 2 * static_cast<size_t>(T));
   }
   L.total = off;
   return L;
@@ -399,7 +408,7 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
 // damping/metric, with the convergence test on the host after every
 // iteration (two reductions read back, as DEER.jl:567-570 does).
 int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const SolveLayout& L,
-              size_t es, size_t smem_fin, int fin_grid) {
+              size_t es, size_t smem_fin, int fin_grid, int init_grid) {
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
@@ -410,7 +419,7 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
                             static_cast<int>(smem_fin)));
   }
   void* init_args[] = {&h->d_params, &h->d_state};
-  CK(cudaLaunchKernel(k.init, dim3(1), dim3(256), init_args, 0, h->stream));
+  CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
   CK(launch_broadcast(h->stream, f64, P.Dp, P.T, P.x0, P.S[0]));
   void* A = ws + L.pA;
   void* B = ws + L.pB;
@@ -467,7 +476,7 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
 // finish + scan sweep kernel; then a logp pass over the returned trajectory.
 int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k, bool coop,
                  const DevParams& P, const SolveLayout& L, size_t es, size_t smem_sweep,
-                 int fin_grid, int64_t Tc) {
+                 int fin_grid, int init_grid, int64_t Tc, bool use_tc) {
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
@@ -482,18 +491,31 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   }
   cublasSetStream(h->cublas, h->stream);
   void* init_args[] = {&h->d_params, &h->d_state};
-  CK(cudaLaunchKernel(k.init, dim3(1), dim3(256), init_args, 0, h->stream));
+  CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
   cudaGraphConditionalHandle none = 0;
   int zero = 0;
   void* sweep_args[] = {&h->d_params, &h->d_state, &none, &zero};
   void *Bb = ws + L.Bb, *Lb = ws + L.Lb, *Gb = ws + L.Gb;
+  int* tc_err = use_tc ? lg_tc_err_word(ws + L.tcws, tg->lg, P.T) : nullptr;
+  if (use_tc) CK(cudaMemsetAsync(tc_err, 0, sizeof(int), h->stream));
+  auto pass = [&](int mode, double* lp) -> int {
+    if (use_tc) {
+      float* G = reinterpret_cast<float*>(ws + L.Gtc);
+      if (lg_tc_pass(h->stream, tg->lg, h->d_params, h->d_state, lp, mode, P.T, ws + L.tcws, G))
+        return 1;
+      if (mode != 2 && lg_mid(h->stream, false, h->d_params, h->d_state, mode + 1, 0,
+                              static_cast<int>(P.T), P.Dp, G) != cudaSuccess)
+        return 1;
+      return 0;
+    }
+    return lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, lp, mode,
+                         P.T, P.Dp, Bb, Lb, Gb, Tc);
+  };
   for (int it = 0; it < P.maxiter; ++it) {
-    if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpx, 0, P.T,
-                      P.Dp, Bb, Lb, Gb, Tc))
+    if (pass(0, P.lpx))
       return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
                   cudaGetErrorString(cudaGetLastError()));
-    if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpy, 1, P.T,
-                      P.Dp, Bb, Lb, Gb, Tc))
+    if (pass(1, P.lpy))
       return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
                   cudaGetErrorString(cudaGetLastError()));
     if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
@@ -511,11 +533,15 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     }
     if (h->h_state->converged || h->h_state->status) break;
   }
-  if (lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.lpx, 2, P.T,
-                    P.Dp, Bb, Lb, Gb, Tc))
-    return fail(h, PMCMC_ERR_CUDA, "logistic logp pass failed");
+  if (pass(2, P.lpx)) return fail(h, PMCMC_ERR_CUDA, "logistic logp pass failed");
   void* fin_args[] = {&h->d_params, &h->d_state};
   CK(cudaLaunchKernel(k.finalize, dim3(fin_grid), dim3(kThreads), fin_args, 0, h->stream));
+  if (use_tc) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, tc_err, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (e) return fail(h, PMCMC_ERR_TIMEOUT, "tensor-core pass: a bounded wait gave up");
+  }
   return PMCMC_OK;
 }
 
@@ -584,8 +610,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (sp_sweep.total > 200 * 1024)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "dimension %lld too large for the fused sweep",
                 (long long)D);
-  const int64_t Tc = logistic ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
-  const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc);
+  const bool use_tc = logistic && !plain && !f64 && lg_tc_supported(tg->lg);
+  const int64_t Tc = logistic && !use_tc ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
+  const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
+                               use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
   unsigned char* ws = h->ws;
@@ -628,6 +656,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   P.agg_b = ws + L.agg_b;
   P.incl = ws + L.incl;
   P.colmax = reinterpret_cast<float*>(ws + L.colmax);
+  P.xi = reinterpret_cast<float*>(ws + L.xi);
+  P.logu = reinterpret_cast<double*>(ws + L.logu);
   if (logistic) {
     for (int i = 0; i < 5; ++i) P.lg[i] = ws + L.lg[i];
     P.lpx = reinterpret_cast<double*>(ws + L.lpx);
@@ -639,7 +669,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
 
   const int fin_grid = static_cast<int>(std::min<int64_t>((T + kWarps - 1) / kWarps,
                                                           int64_t(h->num_sms) * 8));
-  const int init_grid = W < T ? h->num_sms * 4 : 1;
+  const int init_grid = static_cast<int>(
+      std::min<int64_t>((T * (Dp / 4) + 255) / 256, int64_t(h->num_sms) * 8));
   const int64_t nblocks = (N + T - 1) / T;
   std::vector<DevState> states(static_cast<size_t>(nblocks));
   int64_t nsteps = 0;
@@ -658,8 +689,9 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       P.logp_out = logp_out ? ws + L.out_lp : nullptr;
       P.accept_out = accept_out ? ws + L.out_acc : nullptr;
     }
-    rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid, Tc)
-         : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid)
+    rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid,
+                                 init_grid, Tc, use_tc)
+         : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
                   : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
                               init_grid);
     if (rc) return rc;
@@ -886,6 +918,36 @@ int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.X32, x32.data(), 4 * N * Dp, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.y64, y, 8 * N, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.y32, y32.data(), 4 * N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && D <= 256) {
+    // FP16 hi + lo operands for the tensor-core pass
+    const int64_t Dk = D <= 128 ? 128 : 256;
+    const int64_t Np = (N + 127) / 128 * 128;
+    std::vector<__half> xh(static_cast<size_t>(Np * Dk), __float2half(0.f)), xl(xh);
+    for (int64_t n = 0; n < N; ++n)
+      for (int64_t i = 0; i < D; ++i) {
+        const float v = static_cast<float>(X[i * N + n]);
+        const __half hi = __float2half_rn(v);
+        xh[n * Dk + i] = hi;
+        xl[n * Dk + i] = __float2half_rn(v - __half2float(hi));
+      }
+    t->lg.Np = Np;
+    t->lg.Dk = Dk;
+    e = cudaMalloc(&t->lg.Xh, 2 * Np * Dk);
+    if (e == cudaSuccess) e = cudaMalloc(&t->lg.Xl, 2 * Np * Dk);
+    if (e == cudaSuccess) e = cudaMemcpy(t->lg.Xh, xh.data(), 2 * Np * Dk, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->lg.Xl, xl.data(), 2 * Np * Dk, cudaMemcpyHostToDevice);
+    // labels padded to Np for the tensor-core epilogue
+    if (e == cudaSuccess) {
+      float* y32p = nullptr;
+      e = cudaMalloc(&y32p, 4 * Np);
+      if (e == cudaSuccess) e = cudaMemset(y32p, 0, 4 * Np);
+      if (e == cudaSuccess) e = cudaMemcpy(y32p, y32.data(), 4 * N, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) {
+        cudaFree(t->lg.y32);
+        t->lg.y32 = y32p;
+      }
+    }
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     pmcmc_target_destroy(t);
@@ -906,6 +968,8 @@ int pmcmc_target_destroy(pmcmc_target* t) {
   cudaFree(t->lg.X64);
   cudaFree(t->lg.y32);
   cudaFree(t->lg.y64);
+  cudaFree(t->lg.Xh);
+  cudaFree(t->lg.Xl);
   delete t;
   return PMCMC_OK;
 }

@@ -56,6 +56,10 @@ struct DevParams {
   uint8_t* acc_col;
   double* la_col;
   double tau;  // prior precision
+  // tape of the block, written once by the init kernel: xi (T x Dp, FP32,
+  // padded rows zero) and log(u_t) in FP64
+  float* xi;
+  double* logu;
 };
 
 struct DevState {

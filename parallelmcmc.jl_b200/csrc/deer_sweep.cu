@@ -214,7 +214,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     if (4 * j < D) {
       load4(xcol + 4 * j, c.x[q]);
       float n[4];
-      tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), n);
+      load4(P.xi + static_cast<size_t>(t) * Dp + 4 * j, n);
 #pragma unroll
       for (int e = 0; e < 4; ++e) c.xi[q][e] = static_cast<Real>(n[e]);
     } else {
@@ -513,7 +513,7 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
       load4(wp + 4 * j, w[q]);
       load4(hvp + 4 * j, hvy[q]);
       float xi[4];
-      tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), xi);
+      load4(P.xi + off + 4 * j, xi);
       const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t), 0,
                                iter);
       const uint32_t wv = u4_word(pb, (j >> 3) & 3);
@@ -537,7 +537,7 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
     }
   }
   la = warp_sum(la) + (P.lpy[t] - P.lpx[t]);
-  const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+  const double logu = P.logu[t];
   const bool acc = logu < la;
   const double gd = 1.0 / (1.0 + exp(-(la - logu)));
   const Real gp = static_cast<Real>(gd * (1.0 - gd));
@@ -699,7 +699,7 @@ __global__ void __launch_bounds__(kThreads)
       } else {
         Col<Real, QPL> col;
         column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col);
-        const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+        const double logu = P.logu[t];
         const bool acc = logu < col.la;
         const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
         const Real gp = static_cast<Real>(gd * (1.0 - gd));
@@ -946,11 +946,25 @@ __global__ void deer_init_kernel(const DevParams* __restrict__ Pg, DevState* __r
     st->min_margin_bits = 0x7ff0000000000000ull;  // +inf
     st->max_defect_bits = 0;
   }
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  // The block's tape (xi_t, log u_t), generated once and read by every sweep.
+  const TapeKey key(P.seed, P.block);
+  const int64_t nq = P.Dp / 4;
+  for (int64_t i = i0; i < nq * P.T; i += stride) {
+    const int64_t t = i / nq, j = i % nq;
+    float n[4];
+    tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), n);
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (4 * j + e >= P.D) n[e] = 0.f;
+    *reinterpret_cast<float4*>(P.xi + t * P.Dp + 4 * j) = make_float4(n[0], n[1], n[2], n[3]);
+    if (j == 0) P.logu[t] = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+  }
   if (P.W < P.T) {
     const Real* x0 = static_cast<const Real*>(P.x0);
     const int64_t n = P.T * P.Dp;
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int64_t i = i0; i < n; i += stride) {
       const Real v = x0[i % P.Dp];
       static_cast<Real*>(P.S[0])[i] = v;
       static_cast<Real*>(P.S[1])[i] = v;
@@ -986,7 +1000,7 @@ __global__ void __launch_bounds__(kThreads)
     const Real* scol = S + t * Dp;
     Col<Real, QPL> col;
     column_forward<Real, TK, QPL>(P, sm, key, xcol, static_cast<int>(t), col);
-    const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+    const double logu = P.logu[t];
     const bool acc = logu < col.la;
     double def = 0.0, lp = 0.0;
     double* vd = TK == kDenseGauss ? sm.Vd + warp * Dp : nullptr;
@@ -1081,7 +1095,7 @@ __global__ void __launch_bounds__(kThreads)
     const Real* xcol = (t == 0 || from_x0) ? x0 : Sold + (t - 1) * Dp;
     Col<Real, QPL> col;
     column_forward<Real, TK, QPL>(P, sm, key, xcol, static_cast<int>(t), col);
-    const double logu = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+    const double logu = P.logu[t];
     const bool acc = logu < col.la;
     const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
     const Real gp = static_cast<Real>(gd * (1.0 - gd));

@@ -137,7 +137,13 @@ __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* 
     const size_t o = static_cast<size_t>(t) * Dp + 4 * q;
     if (stage == 1) {
       float xi[4];
-      tape_xi4(key, static_cast<uint32_t>(q), static_cast<uint32_t>(t), xi);
+      {
+        const float4 v = *reinterpret_cast<const float4*>(P.xi + t * Dp + 4 * q);
+        xi[0] = v.x;
+        xi[1] = v.y;
+        xi[2] = v.z;
+        xi[3] = v.w;
+      }
       const U4 pb = probe_bits(key, static_cast<uint32_t>(q >> 5), static_cast<uint32_t>(t), 0,
                                iter);
       const uint32_t wv = u4_word(pb, static_cast<int>((q >> 3) & 3));

@@ -3,6 +3,8 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 #include "deer_device.cuh"
@@ -17,11 +19,28 @@ struct LogisticDev {
   float* y32 = nullptr;
   double* y64 = nullptr;
   double tau = 1.0;
+  // tensor-core operands: X as FP16 hi + lo, Np x Dk (rows padded to 128,
+  // columns padded to 128); only built when D <= 256
+  int64_t Np = 0, Dk = 0;
+  __half* Xh = nullptr;
+  __half* Xl = nullptr;
 };
 
 int64_t lg_chunk_cols(int64_t N, int64_t T);
 int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
                   const DevParams* dP, const DevState* dS, double* lp, int mode, int64_t T,
                   int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc);
+
+cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS, int stage,
+                   int64_t t0, int Tc, int64_t Dp, const void* G);
+
+// Tensor-core pass (logistic_tc.cu): mode 0/1/2 as in lg_plain_pass; writes G
+// (Dp x 2T FP32, value block then tangent block) and lp.  ws holds the FP16
+// operand arrays and an error word (lg_tc_ws_bytes).
+bool lg_tc_supported(const LogisticDev& X);
+size_t lg_tc_ws_bytes(const LogisticDev& X, int64_t T);
+int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const DevState* dS,
+               double* lp, int mode, int64_t T, void* ws, float* G);
+int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T);
 
 }  // namespace pmcmc

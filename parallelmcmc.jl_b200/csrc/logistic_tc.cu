@@ -1,0 +1,516 @@
+// logistic_tc.cu -- one logistic-regression pass on the 5th-generation tensor
+// cores (tcgen05 + TMEM + TMA), fused GEMM -> epilogue -> GEMM.
+//
+// For a tile of BT trajectory columns (value columns v_t = x_bar_t or y_t, and
+// the matching tangent columns z_t or w_t) and all N data rows:
+//   GEMM1  L[n, t] = sum_d X[n, d] B[d, t]                     (M = 128 rows of X)
+//   epilogue (per row n, per column t): p = sigmoid(L), r = y_n - p,
+//          s = p (1 - p) L_tangent, loglik = y_n L - softplus(L)  (bayes_logreg.jl:118-154)
+//   GEMM2  G[d, t] += sum_n X[n, d] R[n, t],  R = [r | s]       (M = 128 values of d)
+// The N x 2T intermediate never leaves the SM: L lives in TMEM, R in shared
+// memory, G accumulates in TMEM across all row blocks.  The same shared-memory
+// X tile is GEMM1's K-major A operand and GEMM2's MN-major A operand.
+//
+// Precision: X, the value columns and r are carried as FP16 hi + lo pairs
+// (about 22 significant bits); each value-column product is
+// hi*hi + hi*lo + lo*hi with FP32 accumulation.  Tangent columns (only used
+// for the Jacobian estimate) and s use a single FP16 term.
+//
+// Roles: warps 0-3 (one thread per TMEM lane) run the epilogue; lane 0 of
+// warp 4 issues TMA loads and MMAs and warp 4 owns the TMEM allocation.
+// Every mbarrier wait is bounded; on timeout the kernel records an error,
+// drains its own MMAs and frees TMEM before returning.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "deer_device.cuh"
+#include "logistic.h"
+
+namespace pmcmc {
+namespace tc {
+
+constexpr int BN = 128;  // data rows per block (GEMM1 M)
+constexpr int BT = 32;   // value columns per CTA (plus BT tangent columns)
+constexpr int kThreadsTC = 160;
+constexpr uint32_t kTmemCols = 256;
+constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
+constexpr uint32_t kBoxX = BN * 128;       // one 64-wide d box of X: 128 rows x 128 B
+constexpr uint32_t kBoxB1 = 2 * BT * 128;  // value hi rows | tangent rows
+constexpr uint32_t kBoxBl = BT * 128;      // value lo rows
+constexpr uint32_t kRBlock = (BN / 8) * 128;  // one 8-column block of R: 16 core matrices
+
+struct Layout {
+  uint32_t xh, xl, b1, bl, r, bars, total;
+};
+
+__host__ __device__ inline Layout layout(int nkb) {
+  Layout L;
+  uint32_t off = 0;
+  L.xh = off;
+  off += nkb * kBoxX;
+  L.xl = off;
+  off += nkb * kBoxX;
+  L.b1 = off;
+  off += nkb * kBoxB1;
+  L.bl = off;
+  off += nkb * kBoxBl;
+  L.r = off;
+  off += 12 * kRBlock;
+  L.bars = off;
+  off += 128;
+  L.total = off + 1024;  // slack for 1024-B alignment of the dynamic window
+  return L;
+}
+
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(su32(b))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+          su32(b)),
+      "r"(bytes)
+      : "memory");
+}
+// Bounded wait for the completion of the phase with the given parity: gives up
+// after about a second of SM clock (or at once when another CTA of the launch
+// has already reported an error).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity,
+                                          const volatile int* err) {
+  const uint32_t a = su32(b);
+  const long long start = clock64();
+  for (long long i = 0;; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 255) == 255 && (*err || clock64() - start > kWaitCycles)) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* tm, int x, int y,
+                                       uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(su32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(su32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 32 consecutive FP32 TMEM columns of this warp's 32 lanes (one per thread).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor (tcgen05): start, leading / stride byte
+// offsets, version 1, layout (0 = no swizzle, 2 = 128-byte swizzle).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                          uint32_t layout) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(layout & 7u) << 61;
+  return d;
+}
+
+// Instruction descriptor, kind::f16 with FP16 A/B and FP32 accumulation.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn, bool b_mn) {
+  return (1u << 4) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint4 pack8(const __half (&h)[32], int b) {
+  uint4 u;
+  u.x = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 0])) |
+        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 1])) << 16);
+  u.y = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 2])) |
+        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 3])) << 16);
+  u.z = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 4])) |
+        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 5])) << 16);
+  u.w = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 6])) |
+        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 7])) << 16);
+  return u;
+}
+
+// G (Dp x 2T column-major: value block then tangent block, FP32) and lp (T,
+// FP64) for the column tile blockIdx.x.  has_tangent = 0: value columns only,
+// no G (the logp pass over a returned trajectory).
+__global__ void __launch_bounds__(kThreadsTC, 1)
+    logistic_pass_tc_kernel(const __grid_constant__ CUtensorMap tmXh,
+                            const __grid_constant__ CUtensorMap tmXl,
+                            const __grid_constant__ CUtensorMap tmBh,
+                            const __grid_constant__ CUtensorMap tmBl,
+                            const __grid_constant__ CUtensorMap tmBt,
+                            const float* __restrict__ ylab, int64_t N, int nkb, int64_t T,
+                            int64_t Dp, float* __restrict__ G, double* __restrict__ lp,
+                            int has_tangent, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  const Layout Ly = layout(nkb);
+  unsigned char* sXh = base + Ly.xh;
+  unsigned char* sXl = base + Ly.xl;
+  unsigned char* sB1 = base + Ly.b1;
+  unsigned char* sBl = base + Ly.bl;
+  unsigned char* sR = base + Ly.r;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + Ly.bars);
+  uint64_t* bar_b = bars + 0;  // B tile loaded
+  uint64_t* bar_x = bars + 1;  // X tile loaded
+  uint64_t* bar_l = bars + 2;  // GEMM1 done (L ready)
+  uint64_t* bar_r = bars + 3;  // epilogue wrote R (128 arrivals)
+  uint64_t* bar_g = bars + 4;  // GEMM2 done (X, R free)
+  uint64_t* bar_z = bars + 5;  // teardown drain
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  __shared__ double s_red[4][BT];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * BT;
+  const int nblocks = static_cast<int>((N + BN - 1) / BN);
+  const int nh = nkb / 2;
+  const bool has_g = has_tangent != 0;
+
+  if (threadIdx.x == 0) {
+    mbar_init(bar_b, 1);
+    mbar_init(bar_x, 1);
+    mbar_init(bar_l, 1);
+    mbar_init(bar_r, 128);
+    mbar_init(bar_g, 1);
+    mbar_init(bar_z, 1);
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 4) tmem_alloc(&s_tmem, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t tL = tmem;         // columns [0, 64): value | tangent logits
+  const uint32_t tG = tmem + 64;    // half h at [64 + 64h, 128 + 64h)
+
+  if (warp == 4) {
+    if (lane == 0) {
+      bool ok = true;
+      const uint32_t i1_vt = idesc_f16(128, has_tangent ? 2 * BT : BT, false, false);
+      const uint32_t i1_v = idesc_f16(128, BT, false, false);
+      const uint32_t i2_rs = idesc_f16(128, has_tangent ? 2 * BT : BT, true, true);
+      const uint32_t i2_r = idesc_f16(128, BT, true, true);
+      mbar_expect_tx(bar_b, nkb * (has_tangent ? kBoxB1 : kBoxB1 / 2) + nkb * kBoxBl);
+      for (int kb = 0; kb < nkb; ++kb) {
+        tma_2d(sB1 + kb * kBoxB1, &tmBh, kb * 64, static_cast<int>(t0), bar_b);
+        if (has_tangent) tma_2d(sB1 + kb * kBoxB1 + BT * 128, &tmBt, kb * 64, static_cast<int>(t0), bar_b);
+        tma_2d(sBl + kb * kBoxBl, &tmBl, kb * 64, static_cast<int>(t0), bar_b);
+      }
+      ok = mbar_wait(bar_b, 0, err);
+      int issued = 0;
+      for (int nb = 0; nb < nblocks && ok; ++nb, err) {
+        if (nb > 0 && !(ok = mbar_wait(bar_g, (nb - 1) & 1, err))) break;
+        mbar_expect_tx(bar_x, 2 * nkb * kBoxX);
+        for (int kb = 0; kb < nkb; ++kb) {
+          tma_2d(sXh + kb * kBoxX, &tmXh, kb * 64, nb * BN, bar_x);
+          tma_2d(sXl + kb * kBoxX, &tmXl, kb * 64, nb * BN, bar_x);
+        }
+        if (!(ok = mbar_wait(bar_x, nb & 1, err))) break;
+        tc_fence_after();
+        // GEMM1: L = Xh [Bh | Bt] + Xh Bl + Xl Bh
+        for (int kb = 0; kb < nkb; ++kb)
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t ah = sdesc(su32(sXh + kb * kBoxX) + ks * 32, 16, 1024, 2);
+            const uint64_t al = sdesc(su32(sXl + kb * kBoxX) + ks * 32, 16, 1024, 2);
+            const uint64_t bhz = sdesc(su32(sB1 + kb * kBoxB1) + ks * 32, 16, 1024, 2);
+            const uint64_t bl = sdesc(su32(sBl + kb * kBoxBl) + ks * 32, 16, 1024, 2);
+            mma_f16(tL, ah, bhz, i1_vt, (kb | ks) != 0);
+            mma_f16(tL, ah, bl, i1_v, 1);
+            mma_f16(tL, al, bhz, i1_v, 1);
+          }
+        mma_commit(bar_l);
+        ++issued;
+        if (!(ok = mbar_wait(bar_r, nb & 1, err))) break;
+        tc_fence_after();
+        if (has_g) {
+          // GEMM2: G_h += Xh^T [Rh | S] + Xh^T Rl + Xl^T Rh  (A MN-major, B MN-major)
+          for (int h = 0; h < nh; ++h)
+#pragma unroll
+            for (int kn = 0; kn < BN / 16; ++kn) {
+              const uint64_t ah = sdesc(su32(sXh + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
+              const uint64_t al = sdesc(su32(sXl + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
+              const uint64_t brs = sdesc(su32(sR) + kn * 256, 128, kRBlock, 0);
+              const uint64_t brl = sdesc(su32(sR + 8 * kRBlock) + kn * 256, 128, kRBlock, 0);
+              const uint32_t acc = (nb > 0 || kn > 0) ? 1u : 0u;
+              mma_f16(tG + 64 * h, ah, brs, i2_rs, acc);
+              mma_f16(tG + 64 * h, ah, brl, i2_r, 1);
+              mma_f16(tG + 64 * h, al, brs, i2_r, 1);
+            }
+        }
+        mma_commit(bar_g);
+      }
+      if (!ok) {
+        s_abort = 1;
+        atomicExch(err, 1);
+      }
+      // drain every MMA this thread issued before TMEM is released
+      mma_commit(bar_z);
+      if (!mbar_wait(bar_z, 0, err)) atomicExch(err, 1);
+      (void)issued;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: thread = TMEM lane = data row within the block ----
+    const int row = warp * 32 + lane;
+    const uint32_t lane_off = static_cast<uint32_t>(warp * 32) << 16;
+    double lacc[BT];
+#pragma unroll
+    for (int t = 0; t < BT; ++t) lacc[t] = 0.0;
+    bool ok = true;
+    for (int nb = 0; nb < nblocks; ++nb) {
+      if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
+      tc_fence_after();
+      float v[32], w[32];
+      tmem_ld32(tL + lane_off, v);
+      if (has_tangent) tmem_ld32(tL + lane_off + 32, w);
+      const int64_t n = static_cast<int64_t>(nb) * BN + row;
+      const bool valid = n < N;
+      const float yn = valid ? ylab[n] : 0.f;
+      __half rh[32], rl[32], sh[32];
+#pragma unroll
+      for (int t = 0; t < BT; ++t) {
+        const float l = v[t];
+        const float e = expf(-fabsf(l));
+        const float sp = fmaxf(l, 0.f) + log1pf(e);
+        const float p = l >= 0.f ? 1.f / (1.f + e) : e / (1.f + e);
+        const float r = valid ? yn - p : 0.f;
+        const float s = (valid && has_tangent) ? p * (1.f - p) * w[t] : 0.f;
+        if (valid) lacc[t] += static_cast<double>(yn * l - sp);
+        rh[t] = __float2half_rn(r);
+        rl[t] = __float2half_rn(r - __half2float(rh[t]));
+        sh[t] = __float2half_rn(s);
+      }
+      if (has_g) {
+        const uint32_t roff = static_cast<uint32_t>((row >> 3) * 128 + (row & 7) * 16);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          *reinterpret_cast<uint4*>(sR + (0 + b) * kRBlock + roff) = pack8(rh, b);
+          *reinterpret_cast<uint4*>(sR + (4 + b) * kRBlock + roff) = pack8(sh, b);
+          *reinterpret_cast<uint4*>(sR + (8 + b) * kRBlock + roff) = pack8(rl, b);
+        }
+        fence_async_smem();
+      }
+      tc_fence_before();
+      mbar_arrive(bar_r);
+    }
+    if (ok && has_g && mbar_wait(bar_g, (nblocks - 1) & 1, err)) {
+      tc_fence_after();
+      for (int h = 0; h < nh; ++h) {
+        float gv[32], gt[32];
+        tmem_ld32(tG + 64 * h + lane_off, gv);
+        tmem_ld32(tG + 64 * h + lane_off + 32, gt);
+        const int64_t d = 128 * h + row;
+        if (d < Dp) {
+#pragma unroll
+          for (int t = 0; t < BT; ++t) {
+            if (t0 + t < T) {
+              G[(t0 + t) * Dp + d] = gv[t];
+              G[(T + t0 + t) * Dp + d] = gt[t];
+            }
+          }
+        }
+      }
+    } else if (!ok) {
+      atomicExch(err, 1);
+    }
+#pragma unroll
+    for (int t = 0; t < BT; ++t) {
+      const double s = warp_sum(lacc[t]);
+      if (lane == 0) s_red[warp][t] = s;
+    }
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+    if (threadIdx.x < BT && t0 + threadIdx.x < T)
+      lp[t0 + threadIdx.x] = s_red[0][threadIdx.x] + s_red[1][threadIdx.x] +
+                             s_red[2][threadIdx.x] + s_red[3][threadIdx.x];
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 4) tmem_dealloc(tmem, kTmemCols);
+}
+
+// Builds the FP16 split operands of one pass: Bh/Bl (value columns hi / lo)
+// and Bt (tangent columns), each T x Dk (t-major rows, d contiguous).
+//   mode 0: value x_bar_t, tangent z_t; mode 1: value y_t, tangent w_t;
+//   mode 2: value S_t, no tangent.
+template <typename Real>
+__global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
+                               int mode, int64_t Dk, __half* __restrict__ Bh,
+                               __half* __restrict__ Bl, __half* __restrict__ Bt) {
+  const DevParams& P = *Pg;
+  const int iter = st->iter;
+  const bool from_x0 = iter == 0;
+  const Real* S = static_cast<const Real*>(P.S[st->cur]);
+  const Real* x0 = static_cast<const Real*>(P.x0);
+  const TapeKey key(P.seed, P.block);
+  const int64_t n = P.T * Dk;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t t = i / Dk, d = i % Dk;
+    float v = 0.f, tv = 0.f;
+    if (d < P.D) {
+      if (mode == 0) {
+        v = static_cast<float>((from_x0 || t == 0) ? x0[d] : S[(t - 1) * P.Dp + d]);
+        const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t), 0,
+                                 iter);
+        tv = ((u4_word(pb, static_cast<int>((d >> 5) & 3)) >> (d & 31)) & 1u) ? 1.f : -1.f;
+      } else if (mode == 1) {
+        v = static_cast<float>(static_cast<const Real*>(P.lg[1])[t * P.Dp + d]);
+        tv = static_cast<float>(static_cast<const Real*>(P.lg[2])[t * P.Dp + d]);
+      } else {
+        v = static_cast<float>(S[t * P.Dp + d]);
+      }
+    }
+    const __half h = __float2half_rn(v);
+    Bh[i] = h;
+    Bl[i] = __float2half_rn(v - __half2float(h));
+    if (mode != 2) Bt[i] = __float2half_rn(tv);
+  }
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D FP16 tensor (rows x cols, row-major) with a 64 x box_rows box, 128-B swizzle.
+static bool make_map(CUtensorMap* m, const void* ptr, uint64_t rows, uint64_t cols,
+                     uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {cols * 2};
+  const cuuint32_t box[2] = {64, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+bool lg_tc_supported(const LogisticDev& X) { return X.Xh != nullptr && encode_fn() != nullptr; }
+
+size_t lg_tc_ws_bytes(const LogisticDev& X, int64_t T) {
+  return 3 * static_cast<size_t>(T) * X.Dk * 2 + 1024;
+}
+
+int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T) {
+  return reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(ws) + 3 * T * X.Dk * 2);
+}
+
+int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const DevState* dS,
+               double* lp, int mode, int64_t T, void* ws, float* G_out) {
+  const int64_t Dk = X.Dk;
+  __half* Bh = static_cast<__half*>(ws);
+  __half* Bl = Bh + T * Dk;
+  __half* Bt = Bl + T * Dk;
+  float* G = G_out;
+  int* err = lg_tc_err_word(ws, X, T);
+  const int g = static_cast<int>((T * Dk + 255) / 256 < 148 * 16 ? (T * Dk + 255) / 256 : 148 * 16);
+  tc::tc_prep_kernel<float><<<g, 256, 0, s>>>(dP, dS, mode, Dk, Bh, Bl, Bt);
+  if (cudaGetLastError() != cudaSuccess) return 3;
+  CUtensorMap mXh, mXl, mBh, mBl, mBt;
+  if (!make_map(&mXh, X.Xh, X.Np, Dk, tc::BN) || !make_map(&mXl, X.Xl, X.Np, Dk, tc::BN) ||
+      !make_map(&mBh, Bh, T, Dk, tc::BT) || !make_map(&mBl, Bl, T, Dk, tc::BT) ||
+      !make_map(&mBt, Bt, T, Dk, tc::BT))
+    return 3;
+  const int nkb = static_cast<int>(Dk / 64);
+  const tc::Layout Ly = tc::layout(nkb);
+  cudaFuncSetAttribute(tc::logistic_pass_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(tc::layout(4).total));
+  const int grid = static_cast<int>((T + tc::BT - 1) / tc::BT);
+  tc::logistic_pass_tc_kernel<<<grid, tc::kThreadsTC, Ly.total, s>>>(
+      mXh, mXl, mBh, mBl, mBt, X.y32, X.N, nkb, T, X.Dp, G, lp, mode != 2 ? 1 : 0, err);
+  return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+}  // namespace pmcmc

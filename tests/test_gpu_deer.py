@@ -340,10 +340,12 @@ def _logistic_problem(N, D, seed):
     return X, y
 
 
-@pytest.mark.parametrize("dtype,exec_", [(np.float64, "plain"), (np.float32, "plain"),
-                                         (np.float32, "fused")])
-def test_logistic_matches_sequential(h, dtype, exec_):
-    N, D, T, eps = 300, 12, 256, 0.02
+@pytest.mark.parametrize("dtype,exec_,N,D,T", [
+    (np.float64, "plain", 300, 12, 256), (np.float32, "plain", 300, 12, 256),
+    (np.float32, "fused", 300, 12, 256),     # tensor-core pass, one accumulator half
+    (np.float32, "fused", 777, 200, 96)])    # two halves, padded rows, partial column tile
+def test_logistic_matches_sequential(h, dtype, exec_, N, D, T):
+    eps = 0.02
     X, y = _logistic_problem(N, D, 31)
     model = pmcmc.DensityModel.logistic(X, y)
     sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", dtype=dtype,
