@@ -92,8 +92,13 @@ typedef struct {
   double min_margin;   /* min_t |logalpha_t - log u_t| (FP64) */
   double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory */
   int32_t status;      /* pmcmc_status of the device work */
-  int32_t reserved;
+  int32_t path;        /* PMCMC_PATH_* bits: which kernels ran */
 } pmcmc_info;
+
+#define PMCMC_PATH_FUSED_SWEEP 1  /* one fused kernel per Newton sweep */
+#define PMCMC_PATH_COOPERATIVE 2  /* cooperative sweep (grid-wide carry scan) */
+#define PMCMC_PATH_GRAPH 4        /* Newton loop in a CUDA graph while-node */
+#define PMCMC_PATH_TENSOR_CORE 8  /* logistic passes on tcgen05 tensor cores */
 
 /* ---- handle ------------------------------------------------------------ */
 /* Replaces DEERWorkspace (src/DEER/DEER.jl:47-90): owns all device workspace,

@@ -557,7 +557,6 @@ void fill_info(const DevState& s, pmcmc_info* info) {
   info->min_margin = mm;
   info->max_defect = md;
   info->status = s.status;
-  info->reserved = 0;
 }
 
 int status_error(pmcmc_handle* h, int status) {
@@ -730,6 +729,9 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   }
   agg.status = status;
   if (nblocks == 1) fill_info(states[0], &agg);
+  agg.path = (plain ? 0 : PMCMC_PATH_FUSED_SWEEP) | (tp.coop && !plain ? PMCMC_PATH_COOPERATIVE : 0) |
+             (!plain && !logistic && !h->force_eager && !h->profiling ? PMCMC_PATH_GRAPH : 0) |
+             (use_tc ? PMCMC_PATH_TENSOR_CORE : 0);
   if (info) *info = agg;
   return status_error(h, status);
 }

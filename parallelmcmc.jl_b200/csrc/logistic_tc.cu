@@ -16,8 +16,9 @@
 // hi*hi + hi*lo + lo*hi with FP32 accumulation.  Tangent columns (only used
 // for the Jacobian estimate) and s use a single FP16 term.
 //
-// Roles: warps 0-3 (one thread per TMEM lane) run the epilogue; lane 0 of
-// warp 4 issues TMA loads and MMAs and warp 4 owns the TMEM allocation.
+// Roles: warps 0-7 run the epilogue (warps w and w+4 share TMEM lane quarter
+// w % 4 and split the columns); lane 0 of warp 8 issues TMA loads and MMAs
+// and warp 8 owns the TMEM allocation.
 // Every mbarrier wait is bounded; on timeout the kernel records an error,
 // drains its own MMAs and frees TMEM before returning.
 #include <cuda.h>
@@ -35,7 +36,9 @@ namespace tc {
 
 constexpr int BN = 128;  // data rows per block (GEMM1 M)
 constexpr int BT = 32;   // value columns per CTA (plus BT tangent columns)
-constexpr int kThreadsTC = 160;
+constexpr int kThreadsTC = 288;  // 8 epilogue warps + 1 producer warp
+constexpr int kEpi = 8;
+constexpr int kProd = 8;  // producer / TMEM-owner warp
 constexpr uint32_t kTmemCols = 256;
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
 constexpr uint32_t kBoxX = BN * 128;       // one 64-wide d box of X: 128 rows x 128 B
@@ -165,6 +168,22 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive FP32 TMEM columns of this warp's 32 lanes.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Shared-memory matrix descriptor (tcgen05): start, leading / stride byte
 // offsets, version 1, layout (0 = no swizzle, 2 = 128-byte swizzle).
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
@@ -184,7 +203,8 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn, bool b
          (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-__device__ __forceinline__ uint4 pack8(const __half (&h)[32], int b) {
+template <int NH>
+__device__ __forceinline__ uint4 pack8(const __half (&h)[NH], int b) {
   uint4 u;
   u.x = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 0])) |
         (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 1])) << 16);
@@ -227,7 +247,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   uint64_t* bar_z = bars + 5;  // teardown drain
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
-  __shared__ double s_red[4][BT];
+  __shared__ double s_red[kEpi][BT / 2];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t t0 = static_cast<int64_t>(blockIdx.x) * BT;
@@ -239,13 +259,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     mbar_init(bar_b, 1);
     mbar_init(bar_x, 1);
     mbar_init(bar_l, 1);
-    mbar_init(bar_r, 128);
+    mbar_init(bar_r, 32 * kEpi);
     mbar_init(bar_g, 1);
     mbar_init(bar_z, 1);
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 4) tmem_alloc(&s_tmem, kTmemCols);
+  if (warp == kProd) tmem_alloc(&s_tmem, kTmemCols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -253,7 +273,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   const uint32_t tL = tmem;         // columns [0, 64): value | tangent logits
   const uint32_t tG = tmem + 64;    // half h at [64 + 64h, 128 + 64h)
 
-  if (warp == 4) {
+  if (warp == kProd) {
     if (lane == 0) {
       bool ok = true;
       const uint32_t i1_vt = idesc_f16(128, has_tangent ? 2 * BT : BT, false, false);
@@ -321,32 +341,36 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     }
     __syncwarp();
   } else {
-    // ---- epilogue: thread = TMEM lane = data row within the block ----
-    const int row = warp * 32 + lane;
-    const uint32_t lane_off = static_cast<uint32_t>(warp * 32) << 16;
-    double lacc[BT];
+    // ---- epilogue: thread = TMEM lane = data row; warp half = column half ----
+    const int quarter = warp & 3, half = warp >> 2;  // columns [16 half, 16 half + 16)
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_off = static_cast<uint32_t>(quarter * 32) << 16;
+    constexpr int BH = BT / 2;
+    double lacc[BH];
 #pragma unroll
-    for (int t = 0; t < BT; ++t) lacc[t] = 0.0;
+    for (int t = 0; t < BH; ++t) lacc[t] = 0.0;
     bool ok = true;
+    float y_next = row < N ? __ldg(ylab + row) : 0.f;  // label of this row, one block ahead
     for (int nb = 0; nb < nblocks; ++nb) {
-      if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
-      tc_fence_after();
-      float v[32], w[32];
-      tmem_ld32(tL + lane_off, v);
-      if (has_tangent) tmem_ld32(tL + lane_off + 32, w);
       const int64_t n = static_cast<int64_t>(nb) * BN + row;
       const bool valid = n < N;
-      const float yn = valid ? ylab[n] : 0.f;
-      __half rh[32], rl[32], sh[32];
+      const float yn = y_next;
+      if (n + BN < N) y_next = __ldg(ylab + n + BN);
+      if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
+      tc_fence_after();
+      float v[16], w[16];
+      tmem_ld16(tL + lane_off + BH * half, v);
+      if (has_tangent) tmem_ld16(tL + lane_off + BT + BH * half, w);
+      __half rh[16], rl[16], sh[16];
 #pragma unroll
-      for (int t = 0; t < BT; ++t) {
+      for (int t = 0; t < BH; ++t) {
         const float l = v[t];
-        const float e = expf(-fabsf(l));
-        const float sp = fmaxf(l, 0.f) + log1pf(e);
-        const float p = l >= 0.f ? 1.f / (1.f + e) : e / (1.f + e);
+        const float e = __expf(-fabsf(l));
+        const float inv = __fdividef(1.f, 1.f + e);
+        const float p = l >= 0.f ? inv : e * inv;
         const float r = valid ? yn - p : 0.f;
         const float s = (valid && has_tangent) ? p * (1.f - p) * w[t] : 0.f;
-        if (valid) lacc[t] += static_cast<double>(yn * l - sp);
+        if (valid) lacc[t] += static_cast<double>(yn * l - (fmaxf(l, 0.f) + log1pf(e)));
         rh[t] = __float2half_rn(r);
         rl[t] = __float2half_rn(r - __half2float(rh[t]));
         sh[t] = __float2half_rn(s);
@@ -354,10 +378,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (has_g) {
         const uint32_t roff = static_cast<uint32_t>((row >> 3) * 128 + (row & 7) * 16);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          *reinterpret_cast<uint4*>(sR + (0 + b) * kRBlock + roff) = pack8(rh, b);
-          *reinterpret_cast<uint4*>(sR + (4 + b) * kRBlock + roff) = pack8(sh, b);
-          *reinterpret_cast<uint4*>(sR + (8 + b) * kRBlock + roff) = pack8(rl, b);
+        for (int b = 0; b < 2; ++b) {
+          const int tb = 2 * half + b;  // 8-column block of this thread's columns
+          *reinterpret_cast<uint4*>(sR + (0 + tb) * kRBlock + roff) = pack8(rh, b);
+          *reinterpret_cast<uint4*>(sR + (4 + tb) * kRBlock + roff) = pack8(sh, b);
+          *reinterpret_cast<uint4*>(sR + (8 + tb) * kRBlock + roff) = pack8(rl, b);
         }
         fence_async_smem();
       }
@@ -366,38 +391,38 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     }
     if (ok && has_g && mbar_wait(bar_g, (nblocks - 1) & 1, err)) {
       tc_fence_after();
+      // warp half 0 reads the value block, half 1 the tangent block of G
       for (int h = 0; h < nh; ++h) {
-        float gv[32], gt[32];
-        tmem_ld32(tG + 64 * h + lane_off, gv);
-        tmem_ld32(tG + 64 * h + lane_off + 32, gt);
+        float g[32];
+        tmem_ld32(tG + 64 * h + lane_off + BT * half, g);
         const int64_t d = 128 * h + row;
         if (d < Dp) {
+          const int64_t cbase = half ? T : 0;
 #pragma unroll
-          for (int t = 0; t < BT; ++t) {
-            if (t0 + t < T) {
-              G[(t0 + t) * Dp + d] = gv[t];
-              G[(T + t0 + t) * Dp + d] = gt[t];
-            }
-          }
+          for (int t = 0; t < BT; ++t)
+            if (t0 + t < T) G[(cbase + t0 + t) * Dp + d] = g[t];
         }
       }
     } else if (!ok) {
       atomicExch(err, 1);
     }
 #pragma unroll
-    for (int t = 0; t < BT; ++t) {
-      const double s = warp_sum(lacc[t]);
-      if (lane == 0) s_red[warp][t] = s;
+    for (int t = 0; t < BH; ++t) {
+      const double sum = warp_sum(lacc[t]);
+      if (lane == 0) s_red[warp][t] = sum;
     }
-    asm volatile("bar.sync 1, 128;" ::: "memory");
-    if (threadIdx.x < BT && t0 + threadIdx.x < T)
-      lp[t0 + threadIdx.x] = s_red[0][threadIdx.x] + s_red[1][threadIdx.x] +
-                             s_red[2][threadIdx.x] + s_red[3][threadIdx.x];
+    asm volatile("bar.sync 1, 256;" ::: "memory");
+    if (threadIdx.x < BT && t0 + threadIdx.x < T) {
+      const int t = threadIdx.x, hh = t / BH, tt = t % BH;
+      double a = 0.0;
+      for (int q = 0; q < 4; ++q) a += s_red[4 * hh + q][tt];
+      lp[t0 + t] = a;
+    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 4) tmem_dealloc(tmem, kTmemCols);
+  if (warp == kProd) tmem_dealloc(tmem, kTmemCols);
 }
 
 // Builds the FP16 split operands of one pass: Bh/Bl (value columns hi / lo)

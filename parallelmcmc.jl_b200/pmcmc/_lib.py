@@ -63,11 +63,16 @@ class Info(C.Structure):
     _fields_ = [
         ("iters", C.c_int32), ("converged", C.c_int32), ("metric", C.c_double),
         ("n_accept", C.c_int64), ("min_margin", C.c_double), ("max_defect", C.c_double),
-        ("status", C.c_int32), ("reserved", C.c_int32),
+        ("status", C.c_int32), ("path", C.c_int32),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["path_names"] = [n for b, n in PATH_BITS if self.path & b]
+        return d
+
+
+PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core")]
 
 
 _vp = C.c_void_p

@@ -356,6 +356,7 @@ def test_logistic_matches_sequential(h, dtype, exec_, N, D, T):
     Xi, u = O.tape(8, 0, D, T)
     S_seq, acc_seq, _ = O.mala_sequential(tg, eps, np.zeros(D), Xi, u)
     assert info["converged"], info
+    assert bool(info["path"] & 8) == (exec_ == "fused" and dtype == np.float32 and D <= 256)
     assert np.array_equal(acc, acc_seq)
     # converged to tol_rel = 1e-7: FP64 state sits within ~1e-6 of the fixed point
     assert trace_err(S, S_seq) <= (1e-6 if dtype == np.float64 else 1e-5)
