@@ -99,6 +99,7 @@ typedef struct {
 #define PMCMC_PATH_COOPERATIVE 2  /* cooperative sweep (grid-wide carry scan) */
 #define PMCMC_PATH_GRAPH 4        /* Newton loop in a CUDA graph while-node */
 #define PMCMC_PATH_TENSOR_CORE 8  /* logistic passes on tcgen05 tensor cores */
+#define PMCMC_PATH_FULL_JACOBIAN 16 /* :full mode (dense Jacobian, eigenbasis chunk scan) */
 
 /* ---- handle ------------------------------------------------------------ */
 /* Replaces DEERWorkspace (src/DEER/DEER.jl:47-90): owns all device workspace,
@@ -153,6 +154,36 @@ int pmcmc_deer_solve(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_pa
 int pmcmc_sample(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
                  const void* x0, uint64_t seed, int64_t N, void* vals_out, void* logp_out,
                  uint8_t* accept_out, int32_t mem, pmcmc_info* info);
+
+/* ---- dense-Jacobian mode and the adjoint -------------------------------------
+ * jacobian = PMCMC_JAC_FULL has no counterpart in the reference, which rejects
+ * :full (src/DEER/DEER.jl:465-466, src/interface.jl:274-275).  Here it is
+ * Newton with the exact Jacobian of the surrogate step (the matrix whose action
+ * is the JVP of src/MALA/MALA.jl:768-795), built for the Gaussian targets with
+ * FP32 state, D <= 128 and no sliding window; other requests return
+ * PMCMC_ERR_UNSUPPORTED.
+ *
+ * pmcmc_target_eigen: the eigendecomposition P = Q diag(lam) Q^T of a
+ * Gaussian target's precision that the :full mode and the adjoint work in.
+ * lam has D entries (ascending for the dense target, the given order for the
+ * diagonal one); Q (D x D column-major, may be NULL) holds the eigenvectors.
+ * Host pointers. */
+int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q);
+
+/* pmcmc_deer_adjoint (no counterpart in the reference): gradient of an
+ * objective of a solved trajectory with the accept decisions of that
+ * trajectory held fixed, by one reverse scan.  S is the D x T (FP32)
+ * trajectory returned by pmcmc_deer_solve for the same (p, x0, seed, block),
+ * in `mem`; grad (host, 1 + D doubles) receives dL/depsilon in grad[0] and,
+ * for PMCMC_OBJ_MEAN_SQ, dL/dlog s_i in grad[1 + i] for the covariance
+ * eigenvalues s_i = 1 / lam_i in pmcmc_target_eigen's order (zeros for
+ * PMCMC_OBJ_ESJD).  Objectives:
+ *   PMCMC_OBJ_ESJD     (1/T) sum_t min(1, alpha_t) |y_t - x_{t-1}|^2
+ *   PMCMC_OBJ_MEAN_SQ  (1/T) sum_t |x_t|^2 */
+typedef enum { PMCMC_OBJ_ESJD = 0, PMCMC_OBJ_MEAN_SQ = 1 } pmcmc_objective;
+int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                       const void* x0, uint64_t seed, uint64_t block, const void* S,
+                       int32_t mem, int32_t objective, double* grad);
 
 /* ---- diagonal affine scan ----------------------------------------------------
  * Replaces DEERScan.solve_affine_scan_diag! (src/DEER/DEERScan.jl:102-173):

@@ -130,3 +130,82 @@ def deer_update(tg, eps, s0, S_in, Xi, u, Zs, jacobian="stoch_diag", damping=0.5
     if damping != 1.0:
         S = (1 - damping) * S_in + damping * S
     return S, A, B
+
+
+# ---------------------------------------------------------------------------
+# Objectives of a Gaussian trace and their adjoint (no counterpart in the
+# reference; the checks of the device adjoint).  Target N(mean, P^-1).
+# ---------------------------------------------------------------------------
+
+def gauss_objectives(P, mean, eps, x0, Xi, u):
+    """Sequential FP64 trace (mala_step above) and the two objectives
+    esjd = (1/T) sum_t min(1, alpha_t) |y_t - x_{t-1}|^2 and
+    msq  = (1/T) sum_t |x_t|^2.  Returns (esjd, msq, S, acc)."""
+    P = np.asarray(P, float)
+    tg = NPTarget("dense", P, mean)
+    D, T = Xi.shape
+    S = np.empty((D, T))
+    acc = np.zeros(T, bool)
+    x = np.asarray(x0, float)
+    esjd = 0.0
+    for t in range(T):
+        xi = Xi[:, t].astype(float)
+        gx = tg.grad(x)
+        y = x + eps * gx + np.sqrt(2 * eps) * xi
+        xn, acc[t], la = mala_step(tg, eps, x, xi, float(u[t]))
+        esjd += min(1.0, np.exp(la)) * float((y - x) @ (y - x))
+        x = xn
+        S[:, t] = x
+    return esjd / T, float(np.sum(S * S)) / T, S, acc
+
+
+def gauss_adjoint(P, mean, eps, x0, Xi, u, S, objective, Q=None, s=None):
+    """Adjoint of an objective at the trajectory S with its accept flags held
+    fixed: lambda_t = dL/dx_t + C_{t+1}^T lambda_{t+1}, C = I - eps P (accepted)
+    or I.  Returns (dL/deps, dL/dlog s or None) with P = Q diag(1/s) Q^T."""
+    P = np.asarray(P, float)
+    D, T = S.shape
+    m = np.zeros(D) if mean is None else np.asarray(mean, float)
+    tg = NPTarget("dense", P, m)
+    M = np.eye(D) - eps * P
+    c = np.zeros((D, T))
+    acc = np.zeros(T, bool)
+    direct = 0.0
+    gxs = np.zeros((D, T))
+    for t in range(T):
+        xb = np.asarray(x0, float) if t == 0 else S[:, t - 1]
+        xi = Xi[:, t].astype(float)
+        gx = tg.grad(xb)
+        y = xb + eps * gx + np.sqrt(2 * eps) * xi
+        gy = tg.grad(y)
+        la = (tg.logp(y) + logq(tg, xb, y, gy, eps)) - (tg.logp(xb) + logq(tg, y, xb, gx, eps))
+        acc[t] = np.log(u[t]) < la
+        gxs[:, t] = gx
+        if objective == "mean_sq":
+            c[:, t] += 2.0 * S[:, t] / T
+            continue
+        alpha = min(1.0, np.exp(la))
+        dalpha = alpha if la < 0 else 0.0
+        e2 = float((y - xb) @ (y - xb))
+        dy = gx + xi / np.sqrt(2 * eps)
+        q = xb - y - eps * gy
+        dq = -(M @ dy) - gy
+        dla = gy @ dy - q @ dq / (2 * eps) + (q @ q) / (4 * eps ** 2)
+        direct += (dalpha * dla * e2 + alpha * 2.0 * ((y - xb) @ dy)) / T
+        if t >= 1:
+            v = M @ gy - gx - P @ q + 0.5 * eps * P @ (P @ q)
+            c[:, t - 1] += (dalpha * e2 * v + alpha * 2.0 * eps * (-P @ (y - xb))) / T
+    lam = np.zeros((D, T))
+    lam[:, T - 1] = c[:, T - 1]
+    for t in range(T - 2, -1, -1):
+        lam[:, t] = c[:, t] + ((M @ lam[:, t + 1]) if acc[t + 1] else lam[:, t + 1])
+    geps = direct
+    gls = np.zeros(D) if (Q is not None and objective == "mean_sq") else None
+    for t in range(T):
+        if not acc[t]:
+            continue
+        xb = np.asarray(x0, float) if t == 0 else S[:, t - 1]
+        geps += lam[:, t] @ (gxs[:, t] + Xi[:, t].astype(float) / np.sqrt(2 * eps))
+        if gls is not None:
+            gls += eps / np.asarray(s) * (Q.T @ lam[:, t]) * (Q.T @ (xb - m))
+    return geps, gls

@@ -18,6 +18,7 @@
 #include "../../include/pmcmc_deer.h"
 #include "deer_device.cuh"
 #include "deer_launch.h"
+#include "full.h"
 #include "logistic.h"
 
 using namespace pmcmc;
@@ -58,6 +59,13 @@ struct pmcmc_handle {
   bool profiling = false;
   pmcmc_profile prof{};
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // :full mode
+  FullArgs* d_full = nullptr;
+  DevParams* d_params_e = nullptr;  // eigenbasis view of the :full solve
+  cudaGraphExec_t gexec_full = nullptr;
+  cudaGraphConditionalHandle cond_full = 0;
+  unsigned char gkey_full[192] = {};
+  int full_chunks_override = 0;
 };
 
 struct pmcmc_target {
@@ -69,6 +77,22 @@ struct pmcmc_target {
   float* mean_f = nullptr;
   float* prec_f = nullptr;
   LogisticDev lg;
+  // Gaussian targets: host copy of the precision and, once the :full mode or
+  // the adjoint first needs it, its eigendecomposition P = Q diag(lam) Q^T
+  std::vector<double> prec_host;  // D x D column-major (dense) or D (diagonal)
+  bool eig_ready = false;
+  std::vector<double> eig_lam, eig_Q;  // D, D x D column-major
+  float* lam_f = nullptr;              // Dp
+  float* qrm_f = nullptr;              // Dp x Dp, Q row-major
+  float* qcm_f = nullptr;              // Dp x Dp, Q column-major
+  // the same, padded to the :full sweep stride Dq (zero when D > 128)
+  int dq = 0;
+  float* lamq_f = nullptr;   // Dq
+  double* lamq_d = nullptr;  // Dq
+  float* zq_f = nullptr;     // Dq zeros (eigenbasis mean)
+  double* zq_d = nullptr;    // Dq zeros
+  float* qrmq = nullptr;     // Dq x Dq, Q row-major
+  float* qcmq = nullptr;     // Dq x Dq, Q column-major
 };
 
 namespace {
@@ -209,11 +233,14 @@ struct SolveLayout {
   size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
   size_t xi, logu;
   size_t tcws, Gtc;  // tensor-core logistic path
+  size_t fU, fV, fR, facc, fPhi, fbeta, fdin, eS0, eS1, exi, ex0;  // :full mode
+  size_t alam, acterm, aarev, adirect, ascr, aout;                 // adjoint
   size_t total;
 };
 
 SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain,
-                   int64_t N = 0, int64_t Tc = 0, size_t tc_bytes = 0) {
+                   int64_t N = 0, int64_t Tc = 0, size_t tc_bytes = 0,
+                   const FullPlan* fp = nullptr, bool adjoint = false) {
   SolveLayout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -257,6 +284,28 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
   if (tc_bytes) {
     L.tcws = take(tc_bytes);
     L.Gtc = take(4 * Dp * 2 * static_cast<size_t>(T));
+  }
+  if (fp || adjoint) L.facc = take(static_cast<size_t>(T));
+  if (fp) {
+    const int64_t Dq = fp->Dq;
+    L.eS0 = take(4 * T * Dq);
+    L.eS1 = take(4 * T * Dq);
+    L.exi = take(4 * T * Dq);
+    L.ex0 = take(4 * Dq);
+    L.fU = take(4 * T * Dq);
+    L.fV = take(4 * T * Dq);
+    L.fR = take(4 * T * Dq);
+    L.fPhi = take(4 * static_cast<size_t>(fp->nchunks) * Dq * Dq);
+    L.fbeta = take(4 * static_cast<size_t>(fp->nchunks) * Dq);
+    L.fdin = take(4 * static_cast<size_t>(fp->nchunks) * Dq);
+  }
+  if (adjoint) {
+    L.alam = take(4 * T * Dp);
+    L.acterm = take(4 * T * Dp);
+    L.aarev = take(4 * T * Dp);
+    L.adirect = take(8);
+    L.ascr = take(full_adjoint_scratch_bytes(Dp, T));
+    L.aout = take(8 * static_cast<size_t>(D + 1));
   }
   L.total = off;
   return L;
@@ -545,6 +594,325 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   return PMCMC_OK;
 }
 
+// Symmetric eigendecomposition by cyclic Jacobi rotations (Golub & Van Loan,
+// Matrix Computations, sec. 8.5): A (n x n, row-major) is overwritten; on
+// return w holds the eigenvalues ascending and V (row-major) the eigenvectors
+// as columns.
+void jacobi_eigen(int n, std::vector<double>& A, std::vector<double>& w, std::vector<double>& V) {
+  V.assign(static_cast<size_t>(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) V[static_cast<size_t>(i) * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[static_cast<size_t>(i) * n + j]; };
+  auto v = [&](int i, int j) -> double& { return V[static_cast<size_t>(i) * n + j]; };
+  double scale = 0.0;
+  for (double x : A) scale += x * x;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) off += a(p, q) * a(p, q);
+    if (off <= 1e-30 * scale) break;
+    for (int p = 0; p < n; ++p) {
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+        const double tt =
+            (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(tt * tt + 1.0), sn = tt * c;
+        for (int k = 0; k < n; ++k) {
+          const double kp = a(k, p), kq = a(k, q);
+          a(k, p) = c * kp - sn * kq;
+          a(k, q) = sn * kp + c * kq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double pk = a(p, k), qk = a(q, k);
+          a(p, k) = c * pk - sn * qk;
+          a(q, k) = sn * pk + c * qk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double kp = v(k, p), kq = v(k, q);
+          v(k, p) = c * kp - sn * kq;
+          v(k, q) = sn * kp + c * kq;
+        }
+      }
+    }
+  }
+  std::vector<int> ord(static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  w.resize(static_cast<size_t>(n));
+  std::vector<double> Vs(V.size());
+  for (int j = 0; j < n; ++j) {
+    w[j] = a(ord[j], ord[j]);
+    for (int i = 0; i < n; ++i) Vs[static_cast<size_t>(i) * n + j] = v(i, ord[j]);
+  }
+  V.swap(Vs);
+}
+
+// Eigendecomposition of a Gaussian target's precision, on the host in FP64,
+// uploaded once: lam and Q (row-major and column-major) at the target's
+// stride Dp and at the :full sweep stride Dq.  A diagonal target keeps its
+// order with Q = I.
+int ensure_eigen(pmcmc_handle* h, pmcmc_target* t) {
+  if (t->eig_ready) return PMCMC_OK;
+  if (t->kind != kDiagGauss && t->kind != kDenseGauss)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "eigendecomposition is defined for the Gaussian targets");
+  const int64_t D = t->D, Dp = t->Dp;
+  std::vector<double> lam, Qrow;
+  if (t->kind == kDenseGauss) {
+    std::vector<double> A(static_cast<size_t>(D * D));
+    for (int64_t j = 0; j < D; ++j)
+      for (int64_t i = 0; i < D; ++i)  // symmetrised row-major copy of the column-major input
+        A[i * D + j] = 0.5 * (t->prec_host[j * D + i] + t->prec_host[i * D + j]);
+    jacobi_eigen(static_cast<int>(D), A, lam, Qrow);
+  } else {
+    lam = t->prec_host;
+    Qrow.assign(static_cast<size_t>(D * D), 0.0);
+    for (int64_t i = 0; i < D; ++i) Qrow[i * D + i] = 1.0;
+  }
+  t->eig_lam = lam;
+  t->eig_Q.assign(static_cast<size_t>(D * D), 0.0);
+  for (int64_t i = 0; i < D; ++i)
+    for (int64_t k = 0; k < D; ++k) t->eig_Q[k * D + i] = Qrow[i * D + k];
+  DeviceGuard guard(h->device);
+  // layout at stride n: lam (n), Q row-major and column-major (n x n)
+  auto upload = [&](int64_t n, float* lf, double* ld, float* qr, float* qc) -> int {
+    std::vector<float> lv(static_cast<size_t>(n), 0.f), rv(static_cast<size_t>(n * n), 0.f),
+        cv(static_cast<size_t>(n * n), 0.f);
+    std::vector<double> ldv(static_cast<size_t>(n), 0.0);
+    for (int64_t i = 0; i < D; ++i) {
+      lv[i] = static_cast<float>(lam[i]);
+      ldv[i] = lam[i];
+      for (int64_t k = 0; k < D; ++k) {
+        const float q = static_cast<float>(Qrow[i * D + k]);  // component i of eigenvector k
+        rv[i * n + k] = q;
+        cv[k * n + i] = q;
+      }
+    }
+    CK(cudaMemcpy(lf, lv.data(), 4 * n, cudaMemcpyHostToDevice));
+    if (ld) CK(cudaMemcpy(ld, ldv.data(), 8 * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(qr, rv.data(), 4 * n * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(qc, cv.data(), 4 * n * n, cudaMemcpyHostToDevice));
+    return PMCMC_OK;
+  };
+  if (!t->lam_f) {
+    if (cudaMalloc(&t->lam_f, 4 * Dp) != cudaSuccess ||
+        cudaMalloc(&t->qrm_f, 4 * Dp * Dp) != cudaSuccess ||
+        cudaMalloc(&t->qcm_f, 4 * Dp * Dp) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, PMCMC_ERR_NOMEM, "eigenbasis allocation failed");
+    }
+  }
+  int rc = upload(Dp, t->lam_f, nullptr, t->qrm_f, t->qcm_f);
+  if (rc) return rc;
+  const int Dq = full_stride(Dp);
+  if (Dq) {
+    if (!t->lamq_f &&
+        (cudaMalloc(&t->lamq_f, 4 * Dq) != cudaSuccess || cudaMalloc(&t->lamq_d, 8 * Dq) != cudaSuccess ||
+         cudaMalloc(&t->zq_f, 4 * Dq) != cudaSuccess || cudaMalloc(&t->zq_d, 8 * Dq) != cudaSuccess ||
+         cudaMalloc(&t->qrmq, 4 * Dq * Dq) != cudaSuccess ||
+         cudaMalloc(&t->qcmq, 4 * Dq * Dq) != cudaSuccess)) {
+      cudaGetLastError();
+      return fail(h, PMCMC_ERR_NOMEM, "eigenbasis allocation failed");
+    }
+    rc = upload(Dq, t->lamq_f, t->lamq_d, t->qrmq, t->qcmq);
+    if (rc) return rc;
+    CK(cudaMemset(t->zq_f, 0, 4 * Dq));
+    CK(cudaMemset(t->zq_d, 0, 8 * Dq));
+    t->dq = Dq;
+  }
+  t->eig_ready = true;
+  return PMCMC_OK;
+}
+
+// The eigenbasis view of a :full solve: the diagonal Gaussian N(0, diag(1/lam))
+// at the sweep stride Dq, with the rotated tape and iterate buffers (Q = I for
+// a diagonal target).
+DevParams eigen_view(const DevParams& P, const pmcmc_target* tg, unsigned char* ws,
+                     const SolveLayout& L) {
+  DevParams Pe = P;
+  Pe.Dp = tg->dq;
+  Pe.prec_f = tg->lamq_f;
+  Pe.prec_d = tg->lamq_d;
+  Pe.mean_f = tg->zq_f;
+  Pe.mean_d = tg->zq_d;
+  Pe.xi = reinterpret_cast<float*>(ws + L.exi);
+  Pe.x0 = ws + L.ex0;
+  Pe.S[0] = ws + L.eS0;
+  Pe.S[1] = ws + L.eS1;
+  Pe.tkind = kDiagGauss;
+  return Pe;
+}
+
+struct FullGraphKey {
+  FullPlan fp;
+  const void* init;
+  const void* fin;
+  int init_grid, fin_grid;
+  size_t smem_fin;
+};
+static_assert(sizeof(FullGraphKey) <= sizeof(pmcmc_handle::gkey_full), "graph key size");
+
+// init -> rotate -> while(eval, chunk, carry, apply) -> finalize, the loop
+// condition set by the last CTA of the apply kernel.
+int build_graph_full(pmcmc_handle* h, const FullGraphKey& key) {
+  unsigned char kb[sizeof(pmcmc_handle::gkey_full)] = {};
+  std::memcpy(kb, &key, sizeof key);
+  if (h->gexec_full && std::memcmp(kb, h->gkey_full, sizeof kb) == 0) return PMCMC_OK;
+  if (h->gexec_full) {
+    cudaGraphExecDestroy(h->gexec_full);
+    h->gexec_full = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond = 0;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(h, PMCMC_ERR_CUDA, "cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(e));
+  }
+  h->cond_full = cond;
+  int one = 1;
+  void* pair_args[] = {&h->d_params, &h->d_state};
+  void* sweep_args[] = {&h->d_params, &h->d_full, &h->d_state, &h->cond_full, &one};
+  cudaKernelNodeParams kp{};
+  kp.func = const_cast<void*>(key.init);
+  kp.gridDim = dim3(key.init_grid);
+  kp.blockDim = dim3(256);
+  kp.kernelParams = pair_args;
+  cudaGraphNode_t n_init, n_rot, n_while, n_fin;
+  e = cudaGraphAddKernelNode(&n_init, g, nullptr, 0, &kp);
+  if (e == cudaSuccess) {
+    cudaKernelNodeParams rp{};
+    rp.func = const_cast<void*>(key.fp.rotate);
+    rp.gridDim = dim3(key.fp.rotate_grid);
+    rp.blockDim = dim3(kThreads);
+    rp.sharedMemBytes = static_cast<unsigned>(key.fp.smem_rotate);
+    rp.kernelParams = sweep_args;
+    e = cudaGraphAddKernelNode(&n_rot, g, &n_init, 1, &rp);
+  }
+  cudaGraphNodeParams cp{};
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&n_while, g, &n_rot, 1, &cp);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const void* fns[4] = {key.fp.eval, key.fp.chunk, key.fp.carry, key.fp.apply};
+    const size_t sm[4] = {key.fp.smem_eval, key.fp.smem_chunk, key.fp.smem_carry,
+                          key.fp.smem_apply};
+    const int grid[4] = {key.fp.eval_grid, key.fp.nchunks, 1, key.fp.nchunks};
+    const int thr[4] = {kThreads, key.fp.threads_chunk, 256, kThreads};
+    cudaGraphNode_t prev = nullptr;
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+      cudaKernelNodeParams sp{};
+      sp.func = const_cast<void*>(fns[i]);
+      sp.gridDim = dim3(grid[i]);
+      sp.blockDim = dim3(thr[i]);
+      sp.sharedMemBytes = static_cast<unsigned>(sm[i]);
+      sp.kernelParams = sweep_args;
+      cudaGraphNode_t n;
+      e = cudaGraphAddKernelNode(&n, body, prev ? &prev : nullptr, prev ? 1 : 0, &sp);
+      prev = n;
+    }
+  }
+  if (e == cudaSuccess) {
+    cudaKernelNodeParams fp{};
+    fp.func = const_cast<void*>(key.fin);
+    fp.gridDim = dim3(key.fin_grid);
+    fp.blockDim = dim3(kThreads);
+    fp.sharedMemBytes = static_cast<unsigned>(key.smem_fin);
+    fp.kernelParams = pair_args;
+    e = cudaGraphAddKernelNode(&n_fin, g, &n_while, 1, &fp);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->gexec_full, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->gexec_full = nullptr;
+    return fail(h, PMCMC_ERR_CUDA, "CUDA graph construction failed: %s", cudaGetErrorString(e));
+  }
+  std::memcpy(h->gkey_full, kb, sizeof kb);
+  return PMCMC_OK;
+}
+
+// One DEER block in :full mode (FP32 Gaussian targets).
+int run_full(pmcmc_handle* h, const SweepKernels& k, const FullPlan& fp, const DevParams& P,
+             const DevParams& Pe, const FullArgs& F, size_t smem_fin, int fin_grid,
+             int init_grid) {
+  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_params_e, &Pe, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_full, &F, sizeof(FullArgs), cudaMemcpyHostToDevice, h->stream));
+  {
+    const void* fns[6] = {fp.eval, fp.chunk, fp.carry, fp.apply, k.finalize, fp.rotate};
+    const size_t sm[6] = {fp.smem_eval, fp.smem_chunk, fp.smem_carry, fp.smem_apply, smem_fin,
+                          fp.smem_rotate};
+    for (int i = 0; i < 6; ++i)
+      if (sm[i] > 48 * 1024)
+        CK(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sm[i])));
+  }
+  if (!h->force_eager && !h->profiling) {
+    FullGraphKey key{};
+    key.fp = fp;
+    key.init = k.init;
+    key.fin = k.finalize;
+    key.init_grid = init_grid;
+    key.fin_grid = fin_grid;
+    key.smem_fin = smem_fin;
+    const int rc = build_graph_full(h, key);
+    if (rc == PMCMC_OK) {
+      CK(cudaGraphLaunch(h->gexec_full, h->stream));
+      return PMCMC_OK;
+    }
+    h->force_eager = true;
+  }
+  void* pair_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), pair_args, 0, h->stream));
+  {
+    cudaGraphConditionalHandle none = 0;
+    int zero = 0;
+    void* rargs[] = {&h->d_params, &h->d_full, &h->d_state, &none, &zero};
+    CK(cudaLaunchKernel(fp.rotate, dim3(fp.rotate_grid), dim3(kThreads), rargs, fp.smem_rotate,
+                        h->stream));
+  }
+  for (int it = 0; it < P.maxiter; ++it) {
+    if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
+    CK(full_sweep(h->stream, fp, h->d_params, h->d_full, h->d_state, 0, 0));
+    if (h->profiling) {
+      CK(cudaEventRecord(h->ev[1], h->stream));
+      CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+      h->prof.sweep_launches += 1;
+      h->prof.sweep_ms += ms;
+      if (h->h_state->converged || h->h_state->status) break;
+      continue;
+    }
+    if ((it & 7) == 7 || it + 1 == P.maxiter) {
+      CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      if (h->h_state->converged || h->h_state->status) break;
+    }
+  }
+  if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
+  CK(cudaLaunchKernel(k.finalize, dim3(fin_grid), dim3(kThreads), pair_args, smem_fin,
+                      h->stream));
+  if (h->profiling) {
+    CK(cudaEventRecord(h->ev[1], h->stream));
+    CK(cudaEventSynchronize(h->ev[1]));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    h->prof.finalize_launches += 1;
+    h->prof.finalize_ms += ms;
+  }
+  return PMCMC_OK;
+}
+
 void fill_info(const DevState& s, pmcmc_info* info) {
   if (!info) return;
   info->iters = s.iter;
@@ -586,8 +954,6 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     if (p->window > 0 && p->window < p->T)
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: no sliding window");
   }
-  if (p->jacobian == PMCMC_JAC_FULL)
-    return fail(h, PMCMC_ERR_UNSUPPORTED, ":full jacobian is not built into this library yet");
   DeviceGuard guard(h->device);
   const bool f64 = p->dtype == PMCMC_F64;
   const size_t es = f64 ? 8 : 4;
@@ -599,9 +965,21 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (plain && W < T)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "the plain path has no sliding window");
   const bool logistic = tg->kind == kLogistic;
+  const bool full = p->jacobian == PMCMC_JAC_FULL;
+  FullPlan fplan;
+  if (full) {
+    if (f64) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full is built for FP32 state");
+    if (plain) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full has no plain path");
+    if (W < T) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full has no sliding window");
+    if (!full_plan(Dp, T, tg->kind, h->num_sms, h->full_chunks_override, &fplan))
+      return fail(h, PMCMC_ERR_UNSUPPORTED, ":full is built for D <= 128, got %lld",
+                  (long long)D);
+    rc = ensure_eigen(h, const_cast<pmcmc_target*>(tg));
+    if (rc) return rc;
+  }
   const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
                                   : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
-  const TilePlan tp = choose_tile(h, k, f64, Dp, W, dense);
+  const TilePlan tp = full ? TilePlan{} : choose_tile(h, k, f64, Dp, W, dense);
   const int TT = tp.TT;
   const int ntiles = static_cast<int>((W + TT - 1) / TT);
   const SmemPlan sp_sweep = gauss_sweep_smem(f64, Dp, TT, dense);
@@ -612,7 +990,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   const bool use_tc = logistic && !plain && !f64 && lg_tc_supported(tg->lg);
   const int64_t Tc = logistic && !use_tc ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
-                               use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0);
+                               use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
   unsigned char* ws = h->ws;
@@ -665,6 +1043,27 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     P.la_col = reinterpret_cast<double*>(ws + L.la_col);
     P.tau = tg->lg.tau;
   }
+  FullArgs F{};
+  if (full) {
+    F.Pe = h->d_params_e;
+    F.lam = tg->lam_f;
+    F.Qrm = tg->qrm_f;
+    F.Qcm = tg->qcm_f;
+    F.lamQ = tg->lamq_f;
+    F.QrmQ = tg->qrmq;
+    F.QcmQ = tg->qcmq;
+    F.U = reinterpret_cast<float*>(ws + L.fU);
+    F.V = reinterpret_cast<float*>(ws + L.fV);
+    F.R = reinterpret_cast<float*>(ws + L.fR);
+    F.acc = ws + L.facc;
+    F.Phi = reinterpret_cast<float*>(ws + L.fPhi);
+    F.beta = reinterpret_cast<float*>(ws + L.fbeta);
+    F.din = reinterpret_cast<float*>(ws + L.fdin);
+    F.L = fplan.L;
+    F.nchunks = fplan.nchunks;
+    F.rot = dense ? 1 : 0;
+    F.Dq = fplan.Dq;
+  }
 
   const int fin_grid = static_cast<int>(std::min<int64_t>((T + kWarps - 1) / kWarps,
                                                           int64_t(h->num_sms) * 8));
@@ -690,6 +1089,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     }
     rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid,
                                  init_grid, Tc, use_tc)
+         : full   ? run_full(h, k, fplan, P, eigen_view(P, tg, ws, L), F, sp_fin.total,
+                             fin_grid, init_grid)
          : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
                   : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
                               init_grid);
@@ -729,9 +1130,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   }
   agg.status = status;
   if (nblocks == 1) fill_info(states[0], &agg);
-  agg.path = (plain ? 0 : PMCMC_PATH_FUSED_SWEEP) | (tp.coop && !plain ? PMCMC_PATH_COOPERATIVE : 0) |
+  agg.path = (plain || full ? 0 : PMCMC_PATH_FUSED_SWEEP) |
+             (tp.coop && !plain && !full ? PMCMC_PATH_COOPERATIVE : 0) |
              (!plain && !logistic && !h->force_eager && !h->profiling ? PMCMC_PATH_GRAPH : 0) |
-             (use_tc ? PMCMC_PATH_TENSOR_CORE : 0);
+             (use_tc ? PMCMC_PATH_TENSOR_CORE : 0) | (full ? PMCMC_PATH_FULL_JACOBIAN : 0);
   if (info) *info = agg;
   return status_error(h, status);
 }
@@ -760,6 +1162,7 @@ int make_target(pmcmc_handle* h, int kind, int64_t D, const double* mean, const 
     for (int64_t i = 0; i < D; ++i) pd[i] = prec[i];
   }
   std::vector<float> mf(md.begin(), md.end()), pf(pd.begin(), pd.end());
+  t->prec_host.assign(prec, prec + (kind == kDenseGauss ? D * D : D));
   auto cleanup = [&]() {
     cudaFree(t->mean_d);
     cudaFree(t->prec_d);
@@ -816,7 +1219,9 @@ int pmcmc_create(int device, void* stream, pmcmc_handle** out) {
   if (cudaMalloc(&h->d_params, sizeof(DevParams)) != cudaSuccess ||
       cudaMalloc(&h->d_state, sizeof(DevState)) != cudaSuccess ||
       cudaMallocHost(&h->h_state, sizeof(DevState)) != cudaSuccess ||
-      cudaMallocHost(&h->h_red, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMallocHost(&h->h_red, 4 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&h->d_full, sizeof(FullArgs)) != cudaSuccess ||
+      cudaMalloc(&h->d_params_e, sizeof(DevParams)) != cudaSuccess) {
     cudaGetLastError();
     pmcmc_destroy(h);
     return PMCMC_ERR_NOMEM;
@@ -829,6 +1234,8 @@ int pmcmc_create(int device, void* stream, pmcmc_handle** out) {
   h->no_coop = cv && cv[0] == '1';
   const char* tv = std::getenv("PMCMC_TILE_COLS");
   h->tile_override = tv ? std::atoi(tv) : 0;
+  const char* fv = std::getenv("PMCMC_FULL_CHUNKS");
+  h->full_chunks_override = fv ? std::atoi(fv) : 0;
   if (cudaDeviceSynchronize() != cudaSuccess) {
     cudaGetLastError();
     pmcmc_destroy(h);
@@ -843,7 +1250,10 @@ int pmcmc_destroy(pmcmc_handle* h) {
   DeviceGuard guard(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->gexec_full) cudaGraphExecDestroy(h->gexec_full);
   if (h->cublas) cublasDestroy(h->cublas);
+  cudaFree(h->d_full);
+  cudaFree(h->d_params_e);
   cudaFree(h->ws);
   cudaFree(h->scan_ws);
   cudaFree(h->d_params);
@@ -972,6 +1382,12 @@ int pmcmc_target_destroy(pmcmc_target* t) {
   cudaFree(t->lg.y64);
   cudaFree(t->lg.Xh);
   cudaFree(t->lg.Xl);
+  for (void* q : {static_cast<void*>(t->lam_f), static_cast<void*>(t->qrm_f),
+                  static_cast<void*>(t->qcm_f), static_cast<void*>(t->lamq_f),
+                  static_cast<void*>(t->lamq_d), static_cast<void*>(t->zq_f),
+                  static_cast<void*>(t->zq_d), static_cast<void*>(t->qrmq),
+                  static_cast<void*>(t->qcmq)})
+    cudaFree(q);
   delete t;
   return PMCMC_OK;
 }
@@ -1080,6 +1496,104 @@ int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T,
   CK(cudaMemcpyAsync(flags, scr.counter, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flags[1]) return fail(h, PMCMC_ERR_TIMEOUT, "scan look-back wait exceeded its bound");
+  return PMCMC_OK;
+}
+
+int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q) {
+  if (!t || !lam) return PMCMC_ERR_ARGUMENT;
+  const int rc = ensure_eigen(t->h, t);
+  if (rc) return rc;
+  std::memcpy(lam, t->eig_lam.data(), sizeof(double) * t->D);
+  if (Q) std::memcpy(Q, t->eig_Q.data(), sizeof(double) * t->D * t->D);
+  return PMCMC_OK;
+}
+
+int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                       const void* x0, uint64_t seed, uint64_t block, const void* S, int32_t mem,
+                       int32_t objective, double* grad) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0 || !S || !grad) return fail(h, PMCMC_ERR_ARGUMENT, "x0, S and grad must not be NULL");
+  if (mem != PMCMC_MEM_HOST && mem != PMCMC_MEM_DEVICE)
+    return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
+  if (objective != PMCMC_OBJ_ESJD && objective != PMCMC_OBJ_MEAN_SQ)
+    return fail(h, PMCMC_ERR_ARGUMENT, "objective must be PMCMC_OBJ_ESJD or PMCMC_OBJ_MEAN_SQ");
+  if (tg->kind == kLogistic)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for the Gaussian targets");
+  if (p->dtype != PMCMC_F32) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for FP32");
+  const int64_t D = tg->D, Dp = tg->Dp, T = p->T;
+  if (Dp > 128) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for D <= 128");
+  rc = ensure_eigen(h, const_cast<pmcmc_target*>(tg));
+  if (rc) return rc;
+  DeviceGuard guard(h->device);
+  const bool dense = tg->kind == kDenseGauss;
+  const SolveLayout L = layout(D, Dp, T, 1, 4, false, 0, 0, 0, nullptr, true);
+  rc = ensure_ws(h, L.total);
+  if (rc) return rc;
+  unsigned char* ws = h->ws;
+  const cudaMemcpyKind kin =
+      mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemsetAsync(ws + L.x0a, 0, 4 * Dp, h->stream));
+  CK(cudaMemcpyAsync(ws + L.x0a, x0, 4 * D, kin, h->stream));
+  CK(cudaMemsetAsync(ws + L.S0, 0, 4 * T * Dp, h->stream));
+  CK(cudaMemcpy2DAsync(ws + L.S0, 4 * Dp, S, 4 * D, 4 * D, T, kin, h->stream));
+  DevParams P{};
+  P.D = D;
+  P.Dp = Dp;
+  P.T = T;
+  P.W = T;
+  P.eps = p->epsilon;
+  P.sqrt2eps = std::sqrt(2 * p->epsilon);
+  P.inv4eps = 1.0 / (4 * p->epsilon);
+  P.inv2eps = 1.0 / (2 * p->epsilon);
+  P.damping = p->damping;
+  P.tol_abs = p->tol_abs;
+  P.tol_rel = p->tol_rel;
+  P.seed = seed;
+  P.block = block;
+  P.jac = p->jacobian;
+  P.probes = p->probes;
+  P.maxiter = p->maxiter;
+  P.tkind = tg->kind;
+  P.mean_d = tg->mean_d;
+  P.prec_d = tg->prec_d;
+  P.mean_f = tg->mean_f;
+  P.prec_f = tg->prec_f;
+  P.S[0] = ws + L.S0;
+  P.S[1] = ws + L.S1;
+  P.x0 = ws + L.x0a;
+  P.xi = reinterpret_cast<float*>(ws + L.xi);
+  P.logu = reinterpret_cast<double*>(ws + L.logu);
+  FullArgs F{};
+  F.lam = tg->lam_f;
+  F.Qrm = tg->qrm_f;
+  F.Qcm = tg->qcm_f;
+  F.acc = ws + L.facc;
+  F.rot = dense ? 1 : 0;
+  F.lam_adj = reinterpret_cast<float*>(ws + L.alam);
+  F.cterm = reinterpret_cast<float*>(ws + L.acterm);
+  F.arev = reinterpret_cast<float*>(ws + L.aarev);
+  F.direct = reinterpret_cast<double*>(ws + L.adirect);
+  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_full, &F, sizeof(FullArgs), cudaMemcpyHostToDevice, h->stream));
+  const SweepKernels k = gauss_sweep_kernels(false, tg->kind, PMCMC_JAC_DIAG, D);
+  const int init_grid = static_cast<int>(
+      std::min<int64_t>((T * (Dp / 4) + 255) / 256, int64_t(h->num_sms) * 8));
+  void* init_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
+  h->scan_epoch = (h->scan_epoch + 1) & 0x3fffffffu;
+  if (h->scan_epoch == 0) h->scan_epoch = 1;
+  double* out = reinterpret_cast<double*>(ws + L.aout);
+  CK(full_adjoint(h->stream, h->d_params, h->d_full, F, D, Dp, T, tg->kind, h->num_sms,
+                  objective, reinterpret_cast<const float*>(ws + L.S0), out, ws + L.ascr,
+                  h->scan_epoch));
+  uint32_t flags[2] = {0, 0};
+  CK(cudaMemcpyAsync(grad, out, sizeof(double) * (1 + D), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(flags, ws + L.ascr, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flags[1])
+    return fail(h, PMCMC_ERR_TIMEOUT, "adjoint scan look-back wait exceeded its bound");
   return PMCMC_OK;
 }
 

@@ -25,8 +25,9 @@ SYMBOLS = [
     "pmcmc_target_diag_gauss", "pmcmc_target_dense_gauss", "pmcmc_target_logistic",
     "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
-    "pmcmc_affine_scan_diag_noalloc",
+    "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
 ]
+OBJECTIVE = {"esjd": 0, "mean_sq": 1}
 
 
 class ArgumentError(ValueError):
@@ -72,7 +73,8 @@ class Info(C.Structure):
         return d
 
 
-PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core")]
+PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core"),
+             (16, "full_jacobian")]
 
 
 _vp = C.c_void_p
@@ -112,6 +114,9 @@ def load(path: str = LIB_PATH):
                                                      _vp, _vp, _vp]
         L.pmcmc_set_profiling.argtypes = [_vp, C.c_int32]
         L.pmcmc_get_profile.argtypes = [_vp, C.POINTER(Profile), C.c_int32]
+        L.pmcmc_target_eigen.argtypes = [_vp, _vp, _vp]
+        L.pmcmc_deer_adjoint.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
+                                         C.c_uint64, _vp, C.c_int32, C.c_int32, _vp]
         for fn in SYMBOLS:
             if fn not in ("pmcmc_last_error", "pmcmc_abi_version"):
                 getattr(L, fn).restype = C.c_int

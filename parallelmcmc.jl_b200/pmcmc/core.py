@@ -131,6 +131,17 @@ class DensityModel:
         self._dev[key] = (handle, t)
         return t
 
+    def eigen(self, handle: Optional[L.Handle] = None, device: int = 0):
+        """(lam, Q): the precision P = Q diag(lam) Q^T of a Gaussian target as
+        the :full mode and the adjoint use it (ascending lam for the dense
+        target, the given order for the diagonal one)."""
+        h = handle or L.default_handle(device)
+        t = self.device_target(h)
+        lam = np.empty(self.dim)
+        Q = np.empty((self.dim, self.dim), order="F")
+        L.check(L.load().pmcmc_target_eigen(t, lam.ctypes.data, Q.ctypes.data), h.ptr, "eigen")
+        return lam, Q
+
     def __del__(self):
         try:
             for h, t in self._dev.values():
@@ -363,6 +374,38 @@ def solve(model: DensityModel, sampler: ParallelMALASampler, s0, *, seed: int = 
     if return_logp:
         return Sv, info.as_dict(), lp.arr, accepted
     return Sv, info.as_dict()
+
+
+# --------------------------------------------------------------------------- adjoint
+def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objective: str = "esjd",
+            seed: int = 0, block: int = 0, handle: Optional[L.Handle] = None, device: int = 0):
+    """Gradient of an objective of the solved trajectory S (D, T) with the
+    accept decisions of S held fixed (one reverse scan on the device).
+
+    objective "esjd":    (1/T) sum_t min(1, alpha_t) |y_t - x_{t-1}|^2
+    objective "mean_sq": (1/T) sum_t |x_t|^2
+    Returns {"d_epsilon": float, "d_log_s": (D,) or None}; d_log_s is the
+    gradient with respect to the log covariance eigenvalues s_i = 1/lam_i in
+    the order of DensityModel.eigen (mean_sq only)."""
+    if objective not in L.OBJECTIVE:
+        raise ArgumentError("objective must be 'esjd' or 'mean_sq'")
+    h = handle or L.default_handle(device)
+    tgt = model.device_target(h)
+    keep, x0p, mem = _input_vector(s0, model.dim, sampler.dtype, None)
+    if mem == L.MEM_DEVICE:
+        Sc = S.T.contiguous()
+        sp = Sc.data_ptr()
+    else:
+        Sc = np.ascontiguousarray(np.asarray(S).T, dtype=np.float32)
+        sp = Sc.ctypes.data
+    if tuple(Sc.shape) != (int(sampler.T), model.dim):
+        raise DimensionMismatch("S must be D x T")
+    g = np.zeros(model.dim + 1)
+    p = sampler.params()
+    rc = L.load().pmcmc_deer_adjoint(h.ptr, tgt, C.byref(p), x0p, int(seed), int(block), sp, mem,
+                                     L.OBJECTIVE[objective], g.ctypes.data)
+    L.check(rc, h.ptr, "deer_adjoint")
+    return {"d_epsilon": float(g[0]), "d_log_s": g[1:].copy() if objective == "mean_sq" else None}
 
 
 # --------------------------------------------------------------------------- tape
