@@ -15,6 +15,11 @@ flushed between steps), e2e = the same through pmcmc.sample() with host
 buffers, plain_gpu = the unfused reference-structured GPU path, roofline of
 the sweep kernel, cpu_baseline = the FP64 CPU restatement of the reference
 algorithm on this host's cores.
+
+Secondary measurements (not the headline line; 1 GPU):
+    python bench.py --workload logistic_n10k_d256    # N=10000, D=256, T=65536, :stoch_diag
+    python bench.py --workload corr_gauss_d64_full   # D=64, T=8192, :full
+--small shrinks T (logistic 4096, correlated Gaussian 1024) for profiler captures.
 """
 from __future__ import annotations
 
@@ -268,6 +273,9 @@ def run_ours(args):
     min_bytes = 8 * D * T + 4 * T  # what this kernel must move (tape regenerated in registers)
     hbm, src = peaks()
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+    # dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of this workload,
+    # from the ncu capture summarised in profiles/deer_sweep_kernel_aniso_diag_d100.md
+    traffic = 6754048
 
     # ---- end to end through the public API with host buffers
     x0_host = np.asarray(x0, np.float32)
@@ -311,7 +319,7 @@ def run_ours(args):
                           "newton_iters_mean": statistics.mean(i.iters for i in pinfos),
                           "speedup_fused_over_plain": value / world / plain_value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
                          "kernel": "deer_sweep_kernel", "avg_launch_ms": sweep_ms,
                          "alg_bytes_per_launch": alg_bytes,
                          "kernel_min_bytes_per_launch": min_bytes,
@@ -326,6 +334,123 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def run_secondary(args):
+    """Logistic regression (tensor-core contraction passes) or the correlated
+    Gaussian in :full mode: device-timed solves, Newton iterations, accept
+    rate, and the roofline of the dominant kernel."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import pmcmc
+    from pmcmc import _lib as L
+    from pmcmc import configs
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    h = pmcmc.Handle(0, stream=stream.cuda_stream)
+    lib = L.load()
+    logistic = args.workload == "logistic_n10k_d256"
+    if logistic:
+        model, sampler, x0, meta = configs.logistic_n10k_d256(T=4096 if args.small else 65536)
+    else:
+        model, sampler, x0, meta = configs.correlated_gauss_d64(T=1024 if args.small else 8192)
+        # the sampler's default stopping rule (1e-6 + 1e-5 |S|) allows ~1e-5 relative
+        # error in itself; the 1e-5 trace-error bar needs a tighter one
+        sampler.tol_abs, sampler.tol_rel = 1e-7, 1e-6
+    D, T = model.dim, sampler.T
+    tgt = model.device_target(h)
+    x0_dev = torch.from_numpy(np.asarray(x0, np.float32)).to(dev)
+    S_dev = torch.empty((T, D), dtype=torch.float32, device=dev)
+    lp_dev = torch.empty((T,), dtype=torch.float32, device=dev)
+    acc_dev = torch.empty((T,), dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def solve_dev(smp, block):
+        info = L.Info()
+        p = smp.params()
+        rc = lib.pmcmc_deer_solve(h.ptr, tgt, C.byref(p), x0_dev.data_ptr(), meta["seed"], block,
+                                  S_dev.data_ptr(), lp_dev.data_ptr(), acc_dev.data_ptr(),
+                                  L.MEM_DEVICE, C.byref(info))
+        L.check(rc, h.ptr, "deer_solve")
+        return info
+
+    for w in range(args.warmup):
+        solve_dev(sampler, w)
+    torch.cuda.synchronize(dev)
+    ms, infos = [], []
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            infos.append(solve_dev(sampler, 1000 + k))
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+    value = args.steps * T / (sum(ms) / 1e3)
+    iters = statistics.mean(i.iters for i in infos)
+    acc_rate = statistics.mean(i.n_accept / T for i in infos)
+
+    h.set_profiling(True)
+    solve_dev(sampler, 3000)
+    torch.cuda.synchronize(dev)
+    prof = h.profile(reset=True)
+    h.set_profiling(False)
+    hbm, src = peaks()
+    line = {"metric": METRIC, "secondary": True, "value": value, "unit": "samples/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sum(ms) / args.steps, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded NumPy PCG64 + counter-based Philox tape)",
+            "config": {"workload": meta["workload"], "D": D, "T": T, "eps": sampler.epsilon,
+                       "jacobian": sampler.jacobian, "tol_abs": sampler.tol_abs,
+                       "tol_rel": sampler.tol_rel, "newton_iters_mean": iters,
+                       "accept_rate": acc_rate, "path": infos[-1].as_dict()["path_names"]},
+            "clocks": clk.summary()}
+    if logistic:
+        N = meta.get("N_rows", 10_000)
+        pass_ms = prof["pass_ms"] / max(1, prof["pass_launches"])
+        flops = 8.0 * N * D * T  # two GEMMs of 2 N D (2T) per contraction pass
+        try:
+            with open(PEAKS_PATH) as f:
+                tpk, tsrc = float(json.load(f)["bf16_tflops"]), "measured (bf16 dense, burst)"
+        except Exception:
+            tpk, tsrc = 1590.0, "fallback"
+        achieved = flops / (pass_ms / 1e3) / 1e12
+        line["roofline"] = {"bound": "tensor", "kernel": "logistic_pass_tc_kernel (+ mid kernel)",
+                            "achieved": achieved, "peak": tpk, "unit": "TFLOP/s",
+                            "frac": achieved / tpk, "peak_source": tsrc,
+                            "avg_launch_ms": pass_ms, "alg_flops_per_launch": flops,
+                            "executed_mma_flops_per_launch": 2 * flops,
+                            "sweep_ms": prof["sweep_ms"] / max(1, prof["sweep_launches"])}
+    else:
+        sweep_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
+        Dq = 64
+        # eval: S' and xi' read, u', v', r' written; chunk and apply: u', v', r' read;
+        # apply: S and S' read and written; log u and accept flags
+        alg_bytes = 4 * T * (13 * Dq + 2 * D) + 9 * T
+        achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": "full sweep (eval+chunk+carry+apply)",
+                            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                            "frac": achieved / hbm, "peak_source": src, "avg_sweep_ms": sweep_ms,
+                            "alg_bytes_per_sweep": alg_bytes,
+                            "note": "latency-bound: the chunk, carry and replay recursions are sequential"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        solve_dev(sampler, 1000)
+        S = S_dev.cpu().numpy().T.astype(np.float64)
+        acc = acc_dev.cpu().numpy().astype(bool)
+        Xi, u = O.tape(meta["seed"], 1000, D, T)
+        S_seq, acc_seq, _ = O.mala_sequential(O.Target.dense_gauss(model.target["prec"]),
+                                              sampler.epsilon, np.asarray(x0, np.float64), Xi, u)
+        line["parity"] = {"trace_err_vs_fp64": float(np.max(
+            np.linalg.norm(S - S_seq, axis=0) / np.maximum(np.linalg.norm(S_seq, axis=0), 1e-30))),
+            "accept_identical": bool(np.array_equal(acc, acc_seq))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,10 +458,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--workload", default="aniso_diag_d100",
+                    choices=["aniso_diag_d100", "logistic_n10k_d256", "corr_gauss_d64_full"])
+    ap.add_argument("--small", action="store_true",
+                    help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload != "aniso_diag_d100" and args.impl == "ours":
+        run_secondary(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -220,9 +220,11 @@ int pmcmc_affine_scan_diag_noalloc(int32_t dtype, int64_t D, int64_t T, const vo
  * (its benchmarks time whole solves, benchmarks/.../profile_deer_logreg_components.jl). */
 typedef struct {
   int64_t sweep_launches;
-  double sweep_ms;
+  double sweep_ms;      /* one Newton sweep (the fused kernel; the four :full kernels) */
   int64_t finalize_launches;
   double finalize_ms;
+  int64_t pass_launches;
+  double pass_ms;       /* logistic target: one gradient/HVP contraction pass */
 } pmcmc_profile;
 int pmcmc_set_profiling(pmcmc_handle* h, int32_t on);
 int pmcmc_get_profile(pmcmc_handle* h, pmcmc_profile* out, int32_t reset);

@@ -547,7 +547,7 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   void *Bb = ws + L.Bb, *Lb = ws + L.Lb, *Gb = ws + L.Gb;
   int* tc_err = use_tc ? lg_tc_err_word(ws + L.tcws, tg->lg, P.T) : nullptr;
   if (use_tc) CK(cudaMemsetAsync(tc_err, 0, sizeof(int), h->stream));
-  auto pass = [&](int mode, double* lp) -> int {
+  auto pass_impl = [&](int mode, double* lp) -> int {
     if (use_tc) {
       float* G = reinterpret_cast<float*>(ws + L.Gtc);
       if (lg_tc_pass(h->stream, tg->lg, h->d_params, h->d_state, lp, mode, P.T, ws + L.tcws, G))
@@ -559,6 +559,22 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     }
     return lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, lp, mode,
                          P.T, P.Dp, Bb, Lb, Gb, Tc);
+  };
+  auto pass = [&](int mode, double* lp) -> int {
+    if (h->profiling && mode != 2) {
+      // one contraction pass timed on its own (events around it, synchronised)
+      if (cudaEventRecord(h->ev[0], h->stream) != cudaSuccess) return 1;
+      const int rc = pass_impl(mode, lp);
+      float ms = 0;
+      if (rc || cudaEventRecord(h->ev[1], h->stream) != cudaSuccess ||
+          cudaEventSynchronize(h->ev[1]) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]) != cudaSuccess)
+        return 1;
+      h->prof.pass_launches += 1;
+      h->prof.pass_ms += ms;
+      return 0;
+    }
+    return pass_impl(mode, lp);
   };
   for (int it = 0; it < P.maxiter; ++it) {
     if (pass(0, P.lpx))
@@ -1236,6 +1252,15 @@ int pmcmc_create(int device, void* stream, pmcmc_handle** out) {
   h->tile_override = tv ? std::atoi(tv) : 0;
   const char* fv = std::getenv("PMCMC_FULL_CHUNKS");
   h->full_chunks_override = fv ? std::atoi(fv) : 0;
+  // profiler runs: every Newton loop eager, one launch per real sweep
+  const char* pv = std::getenv("PMCMC_PROFILE");
+  if (pv && pv[0] == '1' &&
+      (cudaEventCreate(&h->ev[0]) != cudaSuccess || cudaEventCreate(&h->ev[1]) != cudaSuccess)) {
+    cudaGetLastError();
+    pmcmc_destroy(h);
+    return PMCMC_ERR_CUDA;
+  }
+  h->profiling = pv && pv[0] == '1';
   if (cudaDeviceSynchronize() != cudaSuccess) {
     cudaGetLastError();
     pmcmc_destroy(h);

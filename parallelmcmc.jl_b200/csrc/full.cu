@@ -24,8 +24,8 @@
 //   eval   one warp per column: the diagonal-target forward step in the
 //          eigenbasis, u', v', r' = f'_t - S'_t and the accept flag
 //   chunk  one CTA per chunk of L columns: the chunk's map [Phi'|beta'] as an
-//          augmented DQ x (DQ+1) matrix in registers; four lanes own a column,
-//          whose recursion needs no barrier (column sums by shuffles)
+//          augmented DQ x (DQ+1) matrix in registers; four or eight lanes own a
+//          column, whose recursion needs no barrier (column sums by shuffles)
 //   carry  one CTA: updates entering each chunk, chunk maps streamed through
 //          a cp.async ring
 //   apply  one CTA per chunk: exact replay of the chunk from its entering
@@ -245,17 +245,19 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
-// chunk: the augmented map [Phi' | beta'] of each chunk.  Lanes 4j..4j+3 own
-// column j (j == DQ is beta'), lane q of them rows [q*NR, (q+1)*NR) in
-// registers (NR = DQ / 4).  Per step: w_j = v'^T [Phi'|beta']_{:,j} (two
-// shuffles), then [Phi'|beta'] <- diag(c_t) [Phi'|beta'] + u' w^T + r' e_DQ^T.
+// chunk: the augmented map [Phi' | beta'] of each chunk.  TPC consecutive
+// lanes own column j (j == DQ is beta'), lane q of them rows [q*NR, (q+1)*NR)
+// in registers (NR = DQ / TPC).  Per step: w_j = v'^T [Phi'|beta']_{:,j}
+// (log2 TPC shuffles), then
+// [Phi'|beta'] <- diag(c_t) [Phi'|beta'] + u' w^T + r' e_DQ^T.
 // Padded rows and columns stay zero.
 // ---------------------------------------------------------------------------
-template <int NR>
-__global__ void __launch_bounds__(NR <= 16 ? 288 : 544)
+template <int NR, int TPC>
+__global__ void __launch_bounds__(544)
     full_chunk_kernel(const DevParams* __restrict__, const FullArgs* __restrict__ Fg,
                       DevState* __restrict__ st, cudaGraphConditionalHandle, int use_cond) {
-  constexpr int DQ = 4 * NR;
+  constexpr int DQ = TPC * NR;
+  static_assert(NR % 4 == 0 && (TPC == 4 || TPC == 8), "chunk tiling");
   __shared__ DevParams P;
   __shared__ FullArgs F;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(NR <= 16 ? 288 : 544)
     }
     for (int i = tid; i < nt; i += blockDim.x) as[i] = F.acc[t0 + i];
   }
-  const int j = tid >> 2, q = tid & 3;
+  const int j = tid / TPC, q = tid % TPC;
   const bool active = j <= DQ;
   const bool bcol = j == DQ;
   const int r0 = q * NR;
@@ -312,6 +314,7 @@ __global__ void __launch_bounds__(NR <= 16 ? 288 : 544)
     float w = (a0 + a1) + (a2 + a3);
     w += __shfl_xor_sync(0xffffffffu, w, 1);
     w += __shfl_xor_sync(0xffffffffu, w, 2);
+    if (TPC == 8) w += __shfl_xor_sync(0xffffffffu, w, 4);
     if (as[s]) {  // uniform across the CTA
 #pragma unroll
       for (int k = 0; k < NR / 4; ++k) {
@@ -823,14 +826,19 @@ size_t apply_smem(int Dq, int64_t Dp, int L) {
   return sizeof(float) * (4 * static_cast<size_t>(L) * Dq + static_cast<size_t>(Dq) * Dq + L * Dp) +
          L + 16;
 }
-int carry_stages(int Dq) { return Dq <= 64 ? 4 : 2; }
+int carry_stages(int Dq) { return Dq <= 64 ? 8 : 2; }
 
 size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// lanes per column of the chunk kernel: 8 where NR stays a multiple of 4 and
+// the CTA within 544 threads
+constexpr int chunk_tpc(int DQ) { return (DQ == 32 || DQ == 64) ? 8 : 4; }
+
 template <int DQ>
 void pick_kernels(FullPlan* fp) {
-  constexpr int NST = DQ <= 64 ? 4 : 2;
-  fp->chunk = reinterpret_cast<const void*>(&full_chunk_kernel<DQ / 4>);
+  constexpr int NST = DQ <= 64 ? 8 : 2;
+  constexpr int TPC = chunk_tpc(DQ);
+  fp->chunk = reinterpret_cast<const void*>(&full_chunk_kernel<DQ / TPC, TPC>);
   fp->carry = reinterpret_cast<const void*>(&full_carry_kernel<DQ, NST>);
   fp->apply = reinterpret_cast<const void*>(&full_apply_kernel<DQ>);
   fp->rotate = reinterpret_cast<const void*>(&full_rotate_kernel<DQ>);
@@ -871,7 +879,7 @@ bool full_plan(int64_t Dp, int64_t T, int tkind, int num_sms, int chunks_overrid
   fp->smem_eval = plan_sweep_smem<float>(Dq, 1, false).total;
   fp->eval_grid =
       static_cast<int>(std::min<int64_t>((T + kWarps - 1) / kWarps, int64_t(num_sms) * 4));
-  fp->threads_chunk = ((4 * (Dq + 1) + 31) / 32) * 32;
+  fp->threads_chunk = ((chunk_tpc(Dq) * (Dq + 1) + 31) / 32) * 32;
   fp->eval = reinterpret_cast<const void*>(&full_eval_kernel);
   switch (Dq) {
     case 16: pick_kernels<16>(fp); break;

@@ -57,7 +57,8 @@ class DeerParams(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("sweep_launches", C.c_int64), ("sweep_ms", C.c_double),
-                ("finalize_launches", C.c_int64), ("finalize_ms", C.c_double)]
+                ("finalize_launches", C.c_int64), ("finalize_ms", C.c_double),
+                ("pass_launches", C.c_int64), ("pass_ms", C.c_double)]
 
 
 class Info(C.Structure):
