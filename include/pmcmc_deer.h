@@ -185,6 +185,32 @@ int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_
                        const void* x0, uint64_t seed, uint64_t block, const void* S,
                        int32_t mem, int32_t objective, double* grad);
 
+/* ---- T-split slices (multi-GPU) ------------------------------------------------
+ * One long chain split into contiguous slices of the block, one per rank, with
+ * one exchange per Newton sweep.  The reference solves a block on one device
+ * (src/DEER/DEER.jl:506-595); these entry points run its deer_update! (DEER.jl:
+ * 398-475) on columns [t0, t0 + W) so that a caller can compose the slices'
+ * affine maps across ranks (the associativity of DEERScan.jl:102-173).  Per
+ * sweep, on every rank:
+ *   1. xbar0 = last column of rank r-1's iterate (x0 on rank 0) -- exchanged;
+ *   2. pmcmc_slice_local: A, B on the slice, agg = [prod_t A_t ; b] (2 x D) with
+ *      b the slice scanned from zero;
+ *   3. carry = maps of ranks 0..r-1 applied to x0 in order (s = a .* s + b);
+ *   4. pmcmc_slice_finish: the slice scanned from carry, damped against the
+ *      previous iterate; red = {max|dS|, max|S|} for the caller's max-reduction
+ *      and the convergence test; last_out = the new last column.
+ * pmcmc_slice_result runs the verification pass on the final iterate (accept
+ * flags, logp, S).  Gaussian targets, :diag / :stoch_diag; state dtype and mem
+ * as in pmcmc_deer_solve.  The slice lives in the handle until the next begin. */
+int pmcmc_slice_begin(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                      const void* x0, uint64_t seed, uint64_t block, int64_t t0, int64_t W,
+                      int32_t mem);
+int pmcmc_slice_local(pmcmc_handle* h, const void* xbar0, void* agg, int32_t mem);
+int pmcmc_slice_finish(pmcmc_handle* h, const void* carry_in, void* last_out, double* red,
+                       int32_t mem);
+int pmcmc_slice_result(pmcmc_handle* h, const void* xbar0, void* S_out, void* logp_out,
+                       uint8_t* accept_out, pmcmc_info* info, int32_t mem);
+
 /* ---- diagonal affine scan ----------------------------------------------------
  * Replaces DEERScan.solve_affine_scan_diag! (src/DEER/DEERScan.jl:102-173):
  * S[:,t] = A[:,t] .* S[:,t-1] + B[:,t], S[:,0-1] = s0.  Single-pass

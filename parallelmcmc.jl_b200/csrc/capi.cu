@@ -34,6 +34,19 @@ struct GraphKey {
   }
 };
 
+// One slice [t0, t0 + W) of a block, solved by the T-split Newton iteration
+// (pmcmc_slice_*): the handle keeps the slice's iterate, tape and A/B.
+struct SliceState {
+  bool active = false;
+  const pmcmc_target* tg = nullptr;
+  pmcmc_deer_params p{};
+  DevParams P{};
+  int cur = 0, iter = 0;
+  size_t es = 4;
+  size_t S[2], x0, xbar, carry, ones, A, B, Sloc, Zb, xi, logu, red, scr, out_S, out_lp,
+      out_acc, x_next, total;
+};
+
 struct pmcmc_handle {
   int device = 0;
   int num_sms = 148;
@@ -66,6 +79,7 @@ struct pmcmc_handle {
   cudaGraphConditionalHandle cond_full = 0;
   unsigned char gkey_full[192] = {};
   int full_chunks_override = 0;
+  SliceState slice;
 };
 
 struct pmcmc_target {
@@ -1619,6 +1633,283 @@ int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer
   CK(cudaStreamSynchronize(h->stream));
   if (flags[1])
     return fail(h, PMCMC_ERR_TIMEOUT, "adjoint scan look-back wait exceeded its bound");
+  return PMCMC_OK;
+}
+
+// ---- T-split slices ---------------------------------------------------------
+// A long chain split across ranks: each rank owns columns [t0, t0 + W) of the
+// block and per Newton sweep (1) evaluates A, B from its iterate and its left
+// boundary, (2) scans them locally into the slice's affine map (prod A, b),
+// (3) after the ranks have exchanged maps, rescans from the carried state and
+// damps (DEER.jl:398-475 applied to a slice; the composition of slice maps is
+// the associativity the scan relies on, DEERScan.jl:102-173).
+namespace {
+
+int slice_copy_in(pmcmc_handle* h, void* dst, const void* src, size_t bytes, int32_t mem) {
+  CK(cudaMemcpyAsync(dst, src, bytes,
+                     mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream));
+  return PMCMC_OK;
+}
+int slice_copy_out(pmcmc_handle* h, void* dst, const void* src, size_t bytes, int32_t mem) {
+  CK(cudaMemcpyAsync(dst, src, bytes,
+                     mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     h->stream));
+  return PMCMC_OK;
+}
+
+ScanScratch slice_scratch(pmcmc_handle* h) {
+  SliceState& sl = h->slice;
+  unsigned char* w = h->ws + sl.scr;
+  const int64_t Dp = sl.P.Dp, W = sl.P.T;
+  const int TT = scan_tile_cols(Dp, W);
+  const int64_t nt = (W + TT - 1) / TT;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  ScanScratch scr;
+  scr.counter = reinterpret_cast<uint32_t*>(w);
+  size_t off = 256;
+  scr.flags = reinterpret_cast<uint32_t*>(w + off);
+  off += al(4 * static_cast<size_t>(nt));
+  scr.agg_a = w + off;
+  off += al(sl.es * nt * Dp);
+  scr.agg_b = w + off;
+  off += al(sl.es * nt * Dp);
+  scr.incl = w + off;
+  return scr;
+}
+
+int slice_scan(pmcmc_handle* h, const void* B, const void* s0, void* out) {
+  SliceState& sl = h->slice;
+  ScanScratch scr = slice_scratch(h);
+  h->scan_epoch = (h->scan_epoch + 1) & 0x3fffffffu;
+  if (h->scan_epoch == 0) h->scan_epoch = 1;
+  CK(launch_affine_scan(h->stream, sl.es == 8, sl.P.Dp, sl.P.T, h->ws + sl.A, B, s0, out, scr,
+                        h->scan_epoch));
+  return PMCMC_OK;
+}
+
+}  // namespace
+
+int pmcmc_slice_begin(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                      const void* x0, uint64_t seed, uint64_t block, int64_t t0, int64_t W,
+                      int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0) return fail(h, PMCMC_ERR_ARGUMENT, "x0 must not be NULL");
+  if (tg->kind == kLogistic)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "slices are built for the Gaussian targets");
+  if (p->jacobian == PMCMC_JAC_FULL)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "slices take the diagonal Jacobians");
+  if (t0 < 0 || W < 1 || t0 + W > p->T)
+    return fail(h, PMCMC_ERR_DIMENSION, "slice [t0, t0 + W) must lie inside [0, T)");
+  DeviceGuard guard(h->device);
+  SliceState& sl = h->slice;
+  sl = SliceState{};
+  sl.tg = tg;
+  sl.p = *p;
+  sl.es = p->dtype == PMCMC_F64 ? 8 : 4;
+  const int64_t D = tg->D, Dp = tg->Dp;
+  const size_t es = sl.es;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~size_t(255);
+    return o;
+  };
+  sl.S[0] = take(es * W * Dp);
+  sl.S[1] = take(es * W * Dp);
+  sl.x0 = take(es * Dp);
+  sl.xbar = take(es * Dp);
+  sl.carry = take(es * Dp);
+  sl.ones = take(es * Dp);
+  sl.A = take(es * W * Dp);
+  sl.B = take(es * W * Dp);
+  sl.Sloc = take(es * W * Dp);
+  sl.Zb = take(es * W * Dp);
+  sl.xi = take(4 * W * Dp);
+  sl.logu = take(8 * static_cast<size_t>(W));
+  sl.red = take(4 * sizeof(unsigned long long));
+  sl.scr = take(scan_scratch_bytes(es == 8, Dp, W) + 1024);
+  sl.out_S = take(es * W * D);
+  sl.out_lp = take(es * W);
+  sl.out_acc = take(static_cast<size_t>(W));
+  sl.x_next = take(es * Dp);
+  sl.total = off;
+  rc = ensure_ws(h, sl.total);
+  if (rc) return rc;
+  unsigned char* ws = h->ws;
+  CK(cudaMemsetAsync(ws, 0, sl.total, h->stream));
+  rc = slice_copy_in(h, ws + sl.x0, x0, es * D, mem);
+  if (rc) return rc;
+  std::vector<double> one64(static_cast<size_t>(Dp), 1.0);
+  std::vector<float> one32(static_cast<size_t>(Dp), 1.f);
+  CK(cudaMemcpyAsync(ws + sl.ones, es == 8 ? static_cast<const void*>(one64.data()) : one32.data(),
+                     es * Dp, cudaMemcpyHostToDevice, h->stream));
+  DevParams& P = sl.P;
+  P.D = D;
+  P.Dp = Dp;
+  P.T = W;
+  P.W = W;
+  P.eps = p->epsilon;
+  P.sqrt2eps = std::sqrt(2 * p->epsilon);
+  P.inv4eps = 1.0 / (4 * p->epsilon);
+  P.inv2eps = 1.0 / (2 * p->epsilon);
+  P.damping = p->damping;
+  P.tol_abs = p->tol_abs;
+  P.tol_rel = p->tol_rel;
+  P.seed = seed;
+  P.block = block;
+  P.jac = p->jacobian;
+  P.probes = p->probes;
+  P.maxiter = p->maxiter;
+  P.tkind = tg->kind;
+  P.t_off = static_cast<int32_t>(t0);
+  P.mean_d = tg->mean_d;
+  P.prec_d = tg->prec_d;
+  P.mean_f = tg->mean_f;
+  P.prec_f = tg->prec_f;
+  P.S[0] = ws + sl.S[0];
+  P.S[1] = ws + sl.S[1];
+  P.x0 = ws + sl.xbar;
+  P.xi = reinterpret_cast<float*>(ws + sl.xi);
+  P.logu = reinterpret_cast<double*>(ws + sl.logu);
+  P.ncols_out = W;
+  P.S_out = ws + sl.out_S;
+  P.logp_out = ws + sl.out_lp;
+  P.accept_out = ws + sl.out_acc;
+  P.x_next = ws + sl.x_next;
+  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  const SweepKernels k = gauss_sweep_kernels(es == 8, tg->kind, p->jacobian, D);
+  const int init_grid = static_cast<int>(
+      std::min<int64_t>((W * (Dp / 4) + 255) / 256, int64_t(h->num_sms) * 8));
+  void* init_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
+  // the iterate starts as x0 broadcast over the slice (DEER.jl:538-542)
+  CK(launch_broadcast(h->stream, es == 8, Dp, W, ws + sl.x0, ws + sl.S[0]));
+  CK(cudaStreamSynchronize(h->stream));
+  sl.active = true;
+  return PMCMC_OK;
+}
+
+int pmcmc_slice_local(pmcmc_handle* h, const void* xbar0, void* agg, int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  SliceState& sl = h->slice;
+  if (!sl.active) return fail(h, PMCMC_ERR_ARGUMENT, "no slice: call pmcmc_slice_begin first");
+  if (!xbar0 || !agg) return fail(h, PMCMC_ERR_ARGUMENT, "null buffer");
+  DeviceGuard guard(h->device);
+  unsigned char* ws = h->ws;
+  const int64_t D = sl.P.D, Dp = sl.P.Dp, W = sl.P.T;
+  const size_t es = sl.es;
+  int rc = slice_copy_in(h, ws + sl.xbar, xbar0, es * D, mem);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->d_params, &sl.P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
+  const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
+  if (smem > 48 * 1024)
+    CK(cudaFuncSetAttribute(k.eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(smem)));
+  const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
+                                                      int64_t(h->num_sms) * 8));
+  const void* Sold = ws + sl.S[sl.cur];
+  int it = sl.iter, from_x0 = 0;
+  void* A = ws + sl.A;
+  void* B = ws + sl.B;
+  void* eval_args[] = {&h->d_params, const_cast<void**>(&Sold), &it, &from_x0, &A, &B};
+  CK(cudaLaunchKernel(k.eval, dim3(grid), dim3(kThreads), eval_args, smem, h->stream));
+  // slice map: b = scan(A, B) from 0, prod A = scan(A, 0) from 1 (last columns)
+  rc = slice_scan(h, ws + sl.B, ws + sl.Zb, ws + sl.Sloc);
+  if (rc) return rc;
+  unsigned char* out = static_cast<unsigned char*>(agg);
+  rc = slice_copy_out(h, out + es * D, ws + sl.Sloc + es * (W - 1) * Dp, es * D, mem);
+  if (rc) return rc;
+  rc = slice_scan(h, ws + sl.Zb, ws + sl.ones, ws + sl.Sloc);
+  if (rc) return rc;
+  rc = slice_copy_out(h, out, ws + sl.Sloc + es * (W - 1) * Dp, es * D, mem);
+  if (rc) return rc;
+  uint32_t flags[2] = {0, 0};
+  CK(cudaMemcpyAsync(flags, ws + sl.scr, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flags[1]) return fail(h, PMCMC_ERR_TIMEOUT, "slice scan look-back wait exceeded its bound");
+  return PMCMC_OK;
+}
+
+int pmcmc_slice_finish(pmcmc_handle* h, const void* carry_in, void* last_out, double* red,
+                       int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  SliceState& sl = h->slice;
+  if (!sl.active) return fail(h, PMCMC_ERR_ARGUMENT, "no slice: call pmcmc_slice_begin first");
+  if (!carry_in || !red) return fail(h, PMCMC_ERR_ARGUMENT, "null buffer");
+  DeviceGuard guard(h->device);
+  unsigned char* ws = h->ws;
+  const int64_t D = sl.P.D, Dp = sl.P.Dp, W = sl.P.T;
+  const size_t es = sl.es;
+  int rc = slice_copy_in(h, ws + sl.carry, carry_in, es * D, mem);
+  if (rc) return rc;
+  void* Snew = ws + sl.S[sl.cur ^ 1];
+  rc = slice_scan(h, ws + sl.B, ws + sl.carry, Snew);
+  if (rc) return rc;
+  auto* r = reinterpret_cast<unsigned long long*>(ws + sl.red);
+  CK(launch_damp_metric(h->stream, es == 8, D, Dp, W, ws + sl.S[sl.cur], Snew, sl.P.damping, r));
+  if (last_out) {
+    rc = slice_copy_out(h, last_out, static_cast<unsigned char*>(Snew) + es * (W - 1) * Dp,
+                        es * D, mem);
+    if (rc) return rc;
+  }
+  unsigned long long hr[3] = {0, 0, 0};
+  uint32_t flags[2] = {0, 0};
+  CK(cudaMemcpyAsync(hr, r, sizeof hr, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(flags, ws + sl.scr, sizeof flags, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flags[1]) return fail(h, PMCMC_ERR_TIMEOUT, "slice scan look-back wait exceeded its bound");
+  std::memcpy(&red[0], &hr[0], 8);
+  std::memcpy(&red[1], &hr[1], 8);
+  sl.cur ^= 1;
+  sl.iter += 1;
+  if (hr[2]) return fail(h, PMCMC_ERR_NONFINITE, "non-finite value in the slice iterate");
+  return PMCMC_OK;
+}
+
+int pmcmc_slice_result(pmcmc_handle* h, const void* xbar0, void* S_out, void* logp_out,
+                       uint8_t* accept_out, pmcmc_info* info, int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  SliceState& sl = h->slice;
+  if (!sl.active) return fail(h, PMCMC_ERR_ARGUMENT, "no slice: call pmcmc_slice_begin first");
+  if (!xbar0 || !S_out) return fail(h, PMCMC_ERR_ARGUMENT, "null buffer");
+  DeviceGuard guard(h->device);
+  unsigned char* ws = h->ws;
+  const int64_t D = sl.P.D, Dp = sl.P.Dp, W = sl.P.T;
+  const size_t es = sl.es;
+  int rc = slice_copy_in(h, ws + sl.xbar, xbar0, es * D, mem);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->d_params, &sl.P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  DevState st{};
+  st.cur = sl.cur;
+  st.iter = sl.iter;
+  st.min_margin_bits = 0x7ff0000000000000ull;
+  *h->h_state = st;
+  CK(cudaMemcpyAsync(h->d_state, h->h_state, sizeof(DevState), cudaMemcpyHostToDevice,
+                     h->stream));
+  const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
+  const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
+  if (smem > 48 * 1024)
+    CK(cudaFuncSetAttribute(k.finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(smem)));
+  const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
+                                                      int64_t(h->num_sms) * 8));
+  void* fin_args[] = {&h->d_params, &h->d_state};
+  CK(cudaLaunchKernel(k.finalize, dim3(grid), dim3(kThreads), fin_args, smem, h->stream));
+  rc = slice_copy_out(h, S_out, ws + sl.out_S, es * W * D, mem);
+  if (!rc && logp_out) rc = slice_copy_out(h, logp_out, ws + sl.out_lp, es * W, mem);
+  if (!rc && accept_out) rc = slice_copy_out(h, accept_out, ws + sl.out_acc, W, mem);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (info) {
+    fill_info(*h->h_state, info);
+    info->path = 0;
+  }
   return PMCMC_OK;
 }
 

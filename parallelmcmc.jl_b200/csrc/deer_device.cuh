@@ -27,7 +27,8 @@ struct DevParams {
   double eps, sqrt2eps, inv4eps, inv2eps, damping, tol_abs, tol_rel;
   uint64_t seed, block;
   int32_t jac, probes, maxiter, tile_cols;
-  int32_t ntiles, tkind, out_device, pad0;
+  int32_t ntiles, tkind, out_device;
+  int32_t t_off;  // tape column of local column 0 (a slice of the block; 0 otherwise)
   // target (device copies, both precisions)
   const double* mean_d;
   const double* prec_d;

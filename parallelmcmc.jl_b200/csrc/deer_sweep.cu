@@ -498,12 +498,13 @@ __global__ void deer_init_kernel(const DevParams* __restrict__ Pg, DevState* __r
   for (int64_t i = i0; i < nq * P.T; i += stride) {
     const int64_t t = i / nq, j = i % nq;
     float n[4];
-    tape_xi4(key, static_cast<uint32_t>(j), static_cast<uint32_t>(t), n);
+    const uint32_t tg = static_cast<uint32_t>(t + P.t_off);
+    tape_xi4(key, static_cast<uint32_t>(j), tg, n);
 #pragma unroll
     for (int e = 0; e < 4; ++e)
       if (4 * j + e >= P.D) n[e] = 0.f;
     *reinterpret_cast<float4*>(P.xi + t * P.Dp + 4 * j) = make_float4(n[0], n[1], n[2], n[3]);
-    if (j == 0) P.logu[t] = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t))));
+    if (j == 0) P.logu[t] = log(static_cast<double>(tape_u(key, tg)));
   }
   if (P.W < P.T) {
     const Real* x0 = static_cast<const Real*>(P.x0);
@@ -644,7 +645,8 @@ __global__ void __launch_bounds__(kThreads)
     const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
     const Real gp = static_cast<Real>(gd * (1.0 - gd));
     Real Aq[QPL][4];
-    column_jacobian<Real, TK, JAC, QPL>(P, sm, key, static_cast<int>(t), iter, acc, gp, col, Aq);
+    column_jacobian<Real, TK, JAC, QPL>(P, sm, key, static_cast<int>(t + P.t_off), iter, acc, gp,
+                                         col, Aq);
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
       const int j = lane + 32 * q;

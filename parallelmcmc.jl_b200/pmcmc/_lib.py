@@ -26,6 +26,7 @@ SYMBOLS = [
     "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
+    "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
 ]
 OBJECTIVE = {"esjd": 0, "mean_sq": 1}
 
@@ -116,6 +117,11 @@ def load(path: str = LIB_PATH):
         L.pmcmc_set_profiling.argtypes = [_vp, C.c_int32]
         L.pmcmc_get_profile.argtypes = [_vp, C.POINTER(Profile), C.c_int32]
         L.pmcmc_target_eigen.argtypes = [_vp, _vp, _vp]
+        L.pmcmc_slice_begin.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
+                                        C.c_uint64, C.c_int64, C.c_int64, C.c_int32]
+        L.pmcmc_slice_local.argtypes = [_vp, _vp, _vp, C.c_int32]
+        L.pmcmc_slice_finish.argtypes = [_vp, _vp, _vp, _vp, C.c_int32]
+        L.pmcmc_slice_result.argtypes = [_vp, _vp, _vp, _vp, _vp, C.POINTER(Info), C.c_int32]
         L.pmcmc_deer_adjoint.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
                                          C.c_uint64, _vp, C.c_int32, C.c_int32, _vp]
         for fn in SYMBOLS:
