@@ -19,6 +19,7 @@ algorithm on this host's cores.
 Secondary measurements (not the headline line; 1 GPU):
     python bench.py --workload logistic_n10k_d256    # N=10000, D=256, T=65536, :stoch_diag
     python bench.py --workload corr_gauss_d64_full   # D=64, T=8192, :full
+    python bench.py --workload logistic_fleet        # 32 uneven logistic chains (N, T / 4)
 --small shrinks T (logistic 4096, correlated Gaussian 1024) for profiler captures.
 """
 from __future__ import annotations
@@ -451,6 +452,63 @@ def run_secondary(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fleet(args):
+    """A bounded sample of the uneven logistic fleet (chains 0..n-1 of the
+    512-chain configuration, N and T scaled by 1/4): all chains through
+    pmcmc_fleet_solve on 8 worker streams, and the same chains one at a time."""
+    import numpy as np
+    import torch
+
+    import pmcmc
+    from pmcmc import configs
+
+    n = 8 if args.small else 32
+    chains = configs.logistic_fleet(n_chains=n, scale=0.25)
+    h = pmcmc.Handle(0)
+    total_T = sum(s.T for _, s, *_ in chains)
+    # stiff chains (small D, large N: eps * lambda_max > 2) can diverge in DEER itself,
+    # as the FP64 CPU restatement does on them; their status is reported per chain
+    pmcmc.fleet_solve(chains, workers=8, handle=h, errors="report")  # warm-up
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = pmcmc.fleet_solve(chains, workers=8, handle=h, errors="report")
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    pmcmc.fleet_solve(chains, workers=1, handle=h, errors="report")
+    torch.cuda.synchronize()
+    serial = time.perf_counter() - t0
+    acc = [float(np.mean(r[3])) for r in res]
+    iters = [r[1]["iters"] for r in res]
+    best = min(times)
+    line = {"metric": METRIC, "secondary": True, "value": total_T / best, "unit": "samples/s",
+            "n_gpus": 1, "steps": len(times), "warmup": 1, "ms_per_step": 1e3 * best,
+            "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded NumPy PCG64 per chain + counter-based Philox tape)",
+            "timing": "host wall clock around pmcmc_fleet_solve with device synchronisation "
+                      "(chains run on 8 streams); best of the timed runs",
+            "config": {"workload": f"logistic_fleet_{n}chains_scale0.25", "chains": n,
+                       "D_range": [min(m.dim for m, *_ in chains), max(m.dim for m, *_ in chains)],
+                       "N_range": [min(m.target["X"].shape[0] for m, *_ in chains),
+                                   max(m.target["X"].shape[0] for m, *_ in chains)],
+                       "T_total": total_T, "workers": 8,
+                       "newton_iters": {"min": min(iters), "median": statistics.median(iters),
+                                        "max": max(iters)},
+                       "accept_rate": {"min": min(acc), "median": statistics.median(acc),
+                                       "max": max(acc)},
+                       "converged": sum(r[1]["converged"] for r in res),
+                       "not_converged": sum(1 for r in res
+                                            if not r[1]["converged"] and r[1]["status"] == 0),
+                       "nonfinite": [i for i, r in enumerate(res) if r[1]["status"] == 4]},
+            "one_chain_at_a_time": {"value": total_T / serial, "unit": "samples/s",
+                                    "speedup_fleet": serial / best},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,13 +517,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--workload", default="aniso_diag_d100",
-                    choices=["aniso_diag_d100", "logistic_n10k_d256", "corr_gauss_d64_full"])
+                    choices=["aniso_diag_d100", "logistic_n10k_d256", "corr_gauss_d64_full",
+                             "logistic_fleet"])
     ap.add_argument("--small", action="store_true",
                     help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload != "aniso_diag_d100" and args.impl == "ours":
+    if args.workload == "logistic_fleet" and args.impl == "ours":
+        run_fleet(args)
+    elif args.workload != "aniso_diag_d100" and args.impl == "ours":
         run_secondary(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -185,6 +185,31 @@ int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_
                        const void* x0, uint64_t seed, uint64_t block, const void* S,
                        int32_t mem, int32_t objective, double* grad);
 
+/* ---- fleet of independent chains ---------------------------------------------
+ * Many independent chains of uneven size (D, N, T) on one GPU.  The reference
+ * runs independent chains through AbstractMCMC's MCMCThreads, one chain and
+ * one workspace per thread (test/test-DEER-Interface.jl:300-318).  Here
+ * `workers` worker handles, each with its own stream and workspace, take
+ * chains largest-first (cost ~ D * N * T) so that small chains fill the device
+ * beside the large ones; every chain runs its own Newton loop to its own
+ * convergence (pmcmc_deer_solve semantics: one block of params.T columns).
+ * Targets may be shared by chains (read-only).  Per-chain results land in the
+ * array; the return value is the first failing chain's status, or PMCMC_OK. */
+typedef struct {
+  const pmcmc_target* target;
+  pmcmc_deer_params params;
+  const void* x0;        /* D, dtype, in `mem` */
+  uint64_t seed, block;
+  void* S_out;           /* D x T, in `mem` */
+  void* logp_out;        /* T, may be NULL */
+  uint8_t* accept_out;   /* T, may be NULL */
+  pmcmc_info info;       /* out */
+  int32_t status;        /* out: pmcmc_status of this chain */
+  int32_t pad0;
+} pmcmc_fleet_chain;
+int pmcmc_fleet_solve(pmcmc_handle* h, pmcmc_fleet_chain* chains, int64_t n, int32_t workers,
+                      int32_t mem);
+
 /* ---- T-split slices (multi-GPU) ------------------------------------------------
  * One long chain split into contiguous slices of the block, one per rank, with
  * one exchange per Newton sweep.  The reference solves a block on one device

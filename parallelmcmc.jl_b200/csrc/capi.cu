@@ -12,7 +12,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pmcmc_deer.h"
@@ -80,6 +83,7 @@ struct pmcmc_handle {
   unsigned char gkey_full[192] = {};
   int full_chunks_override = 0;
   SliceState slice;
+  std::vector<pmcmc_handle*> fleet;  // worker handles of pmcmc_fleet_solve (own streams)
 };
 
 struct pmcmc_target {
@@ -187,7 +191,9 @@ int validate(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p)
     return fail(h, PMCMC_ERR_ARGUMENT, "dtype must be PMCMC_F32 or PMCMC_F64");
   if (p->exec != PMCMC_EXEC_FUSED && p->exec != PMCMC_EXEC_PLAIN)
     return fail(h, PMCMC_ERR_ARGUMENT, "exec must be PMCMC_EXEC_FUSED or PMCMC_EXEC_PLAIN");
-  if (t->h != h) return fail(h, PMCMC_ERR_ARGUMENT, "target belongs to another handle");
+  // targets are read-only device data: any handle on the target's device may use them
+  if (t->h != h && t->h->device != h->device)
+    return fail(h, PMCMC_ERR_ARGUMENT, "target lives on another device");
   return PMCMC_OK;
 }
 
@@ -211,8 +217,7 @@ TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t D
     for (int TT = 8; TT <= 256; TT <<= 1) {
       const size_t smem = gauss_sweep_smem(f64, Dp, TT, dense).total;
       if (smem > 200 * 1024) break;
-      cudaFuncSetAttribute(k.sweep_coop, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem));
+      raise_smem_limit(reinterpret_cast<const void*>(k.sweep_coop), smem);
       int nb = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.sweep_coop, kThreads, smem) !=
           cudaSuccess) {
@@ -402,11 +407,9 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
   const void* sweep_fn = coop ? k.sweep_coop : k.sweep;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 48 * 1024)
-    CK(cudaFuncSetAttribute(sweep_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem_sweep)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(sweep_fn), smem_sweep));
   if (smem_fin > 48 * 1024)
-    CK(cudaFuncSetAttribute(k.finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem_fin)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem_fin));
   if (!h->force_eager && !h->profiling) {
     GraphKey key;
     key.sweep = sweep_fn;
@@ -476,10 +479,8 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_fin > 48 * 1024) {
-    CK(cudaFuncSetAttribute(k.finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem_fin)));
-    CK(cudaFuncSetAttribute(k.eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem_fin)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem_fin));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(k.eval), smem_fin));
   }
   void* init_args[] = {&h->d_params, &h->d_state};
   CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
@@ -544,9 +545,7 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 48 * 1024)
-    CK(cudaFuncSetAttribute(coop ? k.sweep_coop : k.sweep,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem_sweep)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(coop ? k.sweep_coop : k.sweep), smem_sweep));
   if (!h->cublas) {
     if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
       return fail(h, PMCMC_ERR_CUDA, "cublasCreate failed");
@@ -880,8 +879,7 @@ int run_full(pmcmc_handle* h, const SweepKernels& k, const FullPlan& fp, const D
                           fp.smem_rotate};
     for (int i = 0; i < 6; ++i)
       if (sm[i] > 48 * 1024)
-        CK(cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sm[i])));
+        CK(raise_smem_limit(reinterpret_cast<const void*>(fns[i]), sm[i]));
   }
   if (!h->force_eager && !h->profiling) {
     FullGraphKey key{};
@@ -1290,6 +1288,7 @@ int pmcmc_destroy(pmcmc_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->gexec_full) cudaGraphExecDestroy(h->gexec_full);
+  for (pmcmc_handle* w : h->fleet) pmcmc_destroy(w);
   if (h->cublas) cublasDestroy(h->cublas);
   cudaFree(h->d_full);
   cudaFree(h->d_params_e);
@@ -1468,6 +1467,59 @@ int pmcmc_sample(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params
                  uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
   if (!h) return PMCMC_ERR_ARGUMENT;
   return solve_blocks(h, t, p, x0, seed, 0, N, vals_out, logp_out, accept_out, mem, info);
+}
+
+// Fleet: many independent chains of uneven size on one GPU.  Worker handles
+// (each with its own stream and workspace) take chains from a queue ordered by
+// estimated cost, largest first, so that small chains fill the device while
+// the large ones run; every chain keeps its own Newton loop and convergence
+// test.  The reference runs independent chains through AbstractMCMC's
+// MCMCThreads, one chain per Julia thread (test/test-DEER-Interface.jl:300-318).
+int pmcmc_fleet_solve(pmcmc_handle* h, pmcmc_fleet_chain* chains, int64_t n, int32_t workers,
+                      int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  if (n < 0 || (n > 0 && !chains)) return fail(h, PMCMC_ERR_ARGUMENT, "null chain array");
+  if (workers < 1 || workers > 64) return fail(h, PMCMC_ERR_ARGUMENT, "workers must be in [1, 64]");
+  if (n == 0) return PMCMC_OK;
+  DeviceGuard guard(h->device);
+  CK(cudaStreamSynchronize(h->stream));
+  while (static_cast<int>(h->fleet.size()) < workers) {
+    pmcmc_handle* w = nullptr;
+    const int rc = pmcmc_create(h->device, nullptr, &w);
+    if (rc) return fail(h, rc, "fleet worker handle creation failed");
+    h->fleet.push_back(w);
+  }
+  std::vector<int64_t> order(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) order[i] = i;
+  auto cost = [&](int64_t i) {
+    const pmcmc_fleet_chain& c = chains[i];
+    const double D = c.target ? static_cast<double>(c.target->D) : 0.0;
+    const double N = c.target && c.target->kind == kLogistic ? static_cast<double>(c.target->N) : 1.0;
+    return D * N * static_cast<double>(c.params.T);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost(a) > cost(b); });
+  std::atomic<int64_t> next{0};
+  std::vector<std::string> msg(static_cast<size_t>(n));
+  auto work = [&](pmcmc_handle* w) {
+    DeviceGuard g(w->device);
+    for (int64_t k = next.fetch_add(1); k < n; k = next.fetch_add(1)) {
+      pmcmc_fleet_chain& c = chains[order[k]];
+      c.info = pmcmc_info{};
+      c.status = c.target ? solve_blocks(w, c.target, &c.params, c.x0, c.seed, c.block,
+                                         c.params.T, c.S_out, c.logp_out, c.accept_out, mem,
+                                         &c.info)
+                          : PMCMC_ERR_ARGUMENT;
+      if (c.status) msg[static_cast<size_t>(order[k])] = c.target ? w->err : "null target";
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 0; i < workers; ++i) pool.emplace_back(work, h->fleet[static_cast<size_t>(i)]);
+  for (std::thread& t : pool) t.join();
+  for (int64_t i = 0; i < n; ++i)
+    if (chains[i].status)
+      return fail(h, chains[i].status, "fleet chain %lld: %s", (long long)i,
+                  msg[static_cast<size_t>(i)].c_str());
+  return PMCMC_OK;
 }
 
 int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T, const void* A,
@@ -1807,8 +1859,7 @@ int pmcmc_slice_local(pmcmc_handle* h, const void* xbar0, void* agg, int32_t mem
   const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
   const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
   if (smem > 48 * 1024)
-    CK(cudaFuncSetAttribute(k.eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(k.eval), smem));
   const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
                                                       int64_t(h->num_sms) * 8));
   const void* Sold = ws + sl.S[sl.cur];
@@ -1893,8 +1944,7 @@ int pmcmc_slice_result(pmcmc_handle* h, const void* xbar0, void* S_out, void* lo
   const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
   const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
   if (smem > 48 * 1024)
-    CK(cudaFuncSetAttribute(k.finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(smem)));
+    CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem));
   const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
                                                       int64_t(h->num_sms) * 8));
   void* fin_args[] = {&h->d_params, &h->d_state};

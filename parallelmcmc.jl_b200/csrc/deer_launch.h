@@ -21,6 +21,11 @@ struct SweepKernels {
   int qpl = 1;
 };
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`, never
+// lowering it: the attribute is global per function, and handles on other
+// host threads (the fleet) launch the same kernels with other sizes.
+cudaError_t raise_smem_limit(const void* fn, size_t bytes);
+
 SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D);
 SweepKernels logistic_sweep_kernels(bool f64, int64_t D);
 SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);

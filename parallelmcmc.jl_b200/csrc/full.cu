@@ -929,7 +929,7 @@ cudaError_t full_adjoint(cudaStream_t s, const DevParams* Pg, const FullArgs* Fg
   const void* tk = dense ? reinterpret_cast<const void*>(&adjoint_terms_kernel<kDenseGauss>)
                          : reinterpret_cast<const void*>(&adjoint_terms_kernel<kDiagGauss>);
   if (st > 48 * 1024) {
-    e = cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(st));
+    e = raise_smem_limit(reinterpret_cast<const void*>(tk), st);
     if (e != cudaSuccess) return e;
   }
   float* Brev = Fh.cterm;
@@ -968,7 +968,7 @@ cudaError_t full_adjoint(cudaStream_t s, const DevParams* Pg, const FullArgs* Fg
   const void* rk = dense ? reinterpret_cast<const void*>(&adjoint_reduce_kernel<kDenseGauss>)
                          : reinterpret_cast<const void*>(&adjoint_reduce_kernel<kDiagGauss>);
   if (sr > 48 * 1024) {
-    e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sr));
+    e = raise_smem_limit(reinterpret_cast<const void*>(rk), sr);
     if (e != cudaSuccess) return e;
   }
   const float* Lrev = Fh.lam_adj;

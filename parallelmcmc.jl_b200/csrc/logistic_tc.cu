@@ -29,6 +29,7 @@
 #include <cstring>
 
 #include "deer_device.cuh"
+#include "deer_launch.h"
 #include "logistic.h"
 
 namespace pmcmc {
@@ -530,8 +531,7 @@ int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const 
     return 3;
   const int nkb = static_cast<int>(Dk / 64);
   const tc::Layout Ly = tc::layout(nkb);
-  cudaFuncSetAttribute(tc::logistic_pass_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(tc::layout(4).total));
+  raise_smem_limit(reinterpret_cast<const void*>(tc::logistic_pass_tc_kernel), tc::layout(4).total);
   const int grid = static_cast<int>((T + tc::BT - 1) / tc::BT);
   tc::logistic_pass_tc_kernel<<<grid, tc::kThreadsTC, Ly.total, s>>>(
       mXh, mXl, mBh, mBl, mBt, X.y32, X.N, nkb, T, X.Dp, G, lp, mode != 2 ? 1 : 0, err);

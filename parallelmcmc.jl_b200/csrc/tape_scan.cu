@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <unordered_map>
 
 #include "deer_device.cuh"
 #include "deer_launch.h"
@@ -118,6 +120,19 @@ __global__ void __launch_bounds__(kThreads)
   if (tid == 0 && s_err) atomicExch(scr.counter + 1, 1u);  // timeout flag
 }
 
+cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, size_t> limit;
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[fn];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(bytes));
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
 int scan_tile_cols(int64_t D, int64_t T) {
   // Largest power of two <= 64 whose tile (A, B, carry) fits 96 KB, reduced
   // while that leaves fewer than ~2 tiles per SM.
@@ -146,15 +161,13 @@ cudaError_t launch_affine_scan(cudaStream_t s, bool f64, int64_t D, int64_t T, c
   if (e != cudaSuccess) return e;
   if (f64) {
     if (smem > 48 * 1024)
-      cudaFuncSetAttribute(affine_scan_kernel<double>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      raise_smem_limit(reinterpret_cast<const void*>(affine_scan_kernel<double>), smem);
     affine_scan_kernel<double><<<ntiles, kThreads, smem, s>>>(
         D, T, TT, static_cast<const double*>(A), static_cast<const double*>(B),
         static_cast<const double*>(s0), static_cast<double*>(S), scr, epoch);
   } else {
     if (smem > 48 * 1024)
-      cudaFuncSetAttribute(affine_scan_kernel<float>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      raise_smem_limit(reinterpret_cast<const void*>(affine_scan_kernel<float>), smem);
     affine_scan_kernel<float><<<ntiles, kThreads, smem, s>>>(
         D, T, TT, static_cast<const float*>(A), static_cast<const float*>(B),
         static_cast<const float*>(s0), static_cast<float*>(S), scr, epoch);

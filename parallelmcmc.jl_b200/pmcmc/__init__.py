@@ -8,8 +8,8 @@ from types import SimpleNamespace
 from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupported,
                    default_handle, load)
 from .core import (Chain, DensityModel, ParallelMALASampler, ParallelMALAState,
-                   ParallelMALATransition, adjoint, sample, solve, solve_affine_scan_diag, step,
-                   tape)
+                   ParallelMALATransition, adjoint, fleet_solve, sample, solve,
+                   solve_affine_scan_diag, step, tape)
 
 # Module-style aliases matching ParallelMCMC.DEER / ParallelMCMC.DEERScan.
 DEER = SimpleNamespace(solve=solve, adjoint=adjoint, solve_affine_scan_diag=solve_affine_scan_diag)
@@ -18,6 +18,7 @@ DEERScan = SimpleNamespace(solve_affine_scan_diag=solve_affine_scan_diag)
 __all__ = [
     "ArgumentError", "DimensionMismatch", "DeviceError", "Unsupported", "Handle",
     "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
-    "ParallelMALAState", "ParallelMALATransition", "adjoint", "sample", "solve", "step", "tape",
+    "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
+    "step", "tape",
     "solve_affine_scan_diag", "DEER", "DEERScan",
 ]

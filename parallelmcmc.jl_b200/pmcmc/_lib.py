@@ -27,6 +27,7 @@ SYMBOLS = [
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
     "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
+    "pmcmc_fleet_solve",
 ]
 OBJECTIVE = {"esjd": 0, "mean_sq": 1}
 
@@ -75,6 +76,13 @@ class Info(C.Structure):
         return d
 
 
+class FleetChain(C.Structure):
+    _fields_ = [("target", C.c_void_p), ("params", DeerParams), ("x0", C.c_void_p),
+                ("seed", C.c_uint64), ("block", C.c_uint64), ("S_out", C.c_void_p),
+                ("logp_out", C.c_void_p), ("accept_out", C.c_void_p), ("info", Info),
+                ("status", C.c_int32), ("pad0", C.c_int32)]
+
+
 PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core"),
              (16, "full_jacobian")]
 
@@ -117,6 +125,8 @@ def load(path: str = LIB_PATH):
         L.pmcmc_set_profiling.argtypes = [_vp, C.c_int32]
         L.pmcmc_get_profile.argtypes = [_vp, C.POINTER(Profile), C.c_int32]
         L.pmcmc_target_eigen.argtypes = [_vp, _vp, _vp]
+        L.pmcmc_fleet_solve.argtypes = [_vp, C.POINTER(FleetChain), C.c_int64, C.c_int32,
+                                        C.c_int32]
         L.pmcmc_slice_begin.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
                                         C.c_uint64, C.c_int64, C.c_int64, C.c_int32]
         L.pmcmc_slice_local.argtypes = [_vp, _vp, _vp, C.c_int32]

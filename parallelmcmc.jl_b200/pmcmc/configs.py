@@ -66,3 +66,26 @@ def correlated_gauss_d64(T=8192, dtype=np.float32, seed=3, jacobian="full"):
     sampler = ParallelMALASampler(0.05, T=T, jacobian=jacobian, dtype=dtype)
     return model, sampler, np.zeros(D, dtype=dtype), {"N": T, "seed": seed, "s": s, "Q": Q,
                                                       "workload": f"corr_gauss_D64_T{T}"}
+
+
+def logistic_fleet(n_chains=512, scale=1.0, dtype=np.float32, first=0):
+    """Uneven fleet of independent logistic-regression chains: chain c (seed c)
+    has D uniform on {16, 32, ..., 512}, N uniform in [1000, 20000], T uniform
+    in [1024, 32768], eps = 0.5 / sqrt(D), :stoch_diag, data from the generative
+    model of logistic_n10k_d256.  `scale` < 1 shrinks N and T (a bounded sample
+    of the fleet); chains first .. first + n_chains - 1.
+    Returns a list of (model, sampler, x0, seed, block)."""
+    out = []
+    for c in range(first, first + n_chains):
+        rng = np.random.default_rng(c)
+        D = int(16 * rng.integers(1, 33))
+        N = max(16, int(rng.integers(1000, 20001) * scale))
+        T = max(16, int(rng.integers(1024, 32769) * scale))
+        X = (rng.standard_normal((N, D)) / np.sqrt(D)).astype(np.float32).astype(np.float64)
+        th = rng.standard_normal(D)
+        y = (rng.random(N) < 1.0 / (1.0 + np.exp(-(X @ th)))).astype(np.float64)
+        model = DensityModel.logistic(X, y, prior_prec=1.0)
+        sampler = ParallelMALASampler(0.5 / np.sqrt(D), T=T, jacobian="stoch_diag", probes=1,
+                                      dtype=dtype)
+        out.append((model, sampler, np.zeros(D, dtype=dtype), c, 0))
+    return out

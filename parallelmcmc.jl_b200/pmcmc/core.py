@@ -408,6 +408,49 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
     return {"d_epsilon": float(g[0]), "d_log_s": g[1:].copy() if objective == "mean_sq" else None}
 
 
+# --------------------------------------------------------------------------- fleet
+def fleet_solve(chains, *, workers: int = 8, handle: Optional[L.Handle] = None, device: int = 0,
+                errors: str = "raise"):
+    """Many independent chains of uneven size on one GPU (MCMCThreads-style):
+    `chains` is a list of (model, sampler, x0, seed, block) tuples, one DEER
+    block of sampler.T columns each.  Worker streams take chains largest-first;
+    every chain converges on its own.  Returns a list of (S (D, T), info,
+    logp (T,), accept (T,)); info["status"] is the chain's pmcmc status.
+    errors="raise" raises for the first failing chain (after all chains ran);
+    errors="report" returns every chain's result with its status."""
+    if errors not in ("raise", "report"):
+        raise ArgumentError("errors must be 'raise' or 'report'")
+    h = handle or L.default_handle(device)
+    arr = (L.FleetChain * len(chains))()
+    keep = []
+    outs = []
+    for i, (model, sampler, x0, seed, block) in enumerate(chains):
+        dt = sampler.dtype
+        x = np.ascontiguousarray(np.asarray(x0, dtype=dt).ravel())
+        if x.size != model.dim:
+            raise DimensionMismatch(f"chain {i}: initial state must have length {model.dim}")
+        T = int(sampler.T)
+        S = np.empty((T, model.dim), dt)
+        lp = np.empty(T, dt)
+        acc = np.empty(T, np.uint8)
+        keep.append(x)
+        outs.append((S, lp, acc))
+        c = arr[i]
+        c.target = model.device_target(h)
+        c.params = sampler.params()
+        c.x0, c.seed, c.block = x.ctypes.data, int(seed), int(block)
+        c.S_out, c.logp_out, c.accept_out = S.ctypes.data, lp.ctypes.data, acc.ctypes.data
+    rc = L.load().pmcmc_fleet_solve(h.ptr, arr, len(chains), int(workers), L.MEM_HOST)
+    if errors == "raise" or rc not in (L.OK, L.ERR_NONFINITE, L.ERR_TIMEOUT):
+        L.check(rc, h.ptr, "fleet_solve")
+    res = []
+    for i, (S, lp, acc) in enumerate(outs):
+        info = arr[i].info.as_dict()
+        info["status"] = int(arr[i].status)
+        res.append((S.T, info, lp, acc.astype(bool)))
+    return res
+
+
 # --------------------------------------------------------------------------- tape
 def tape(D: int, T: int, seed: int, block: int = 0, *, handle: Optional[L.Handle] = None,
          device: int = 0):

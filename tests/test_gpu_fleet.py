@@ -1,0 +1,39 @@
+"""Fleet of independent chains (pmcmc_fleet_solve) against the same chains
+solved one at a time: every chain takes the same kernels on its own worker
+stream, so trajectories agree to 1e-6 relative, accept flags and iteration
+counts are equal."""
+import numpy as np
+import pytest
+
+import pmcmc
+from pmcmc import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fleet_matches_chains_solved_one_by_one():
+    chains = configs.logistic_fleet(n_chains=6, scale=0.05)
+    # a Gaussian chain in the same fleet
+    g = pmcmc.DensityModel.diag_gaussian(10 ** np.random.default_rng(1).uniform(-1, 1, 20))
+    chains.append((g, pmcmc.ParallelMALASampler(0.05, T=700, jacobian="diag", dtype=np.float32),
+                   np.zeros(20, np.float32), 11, 0))
+    h = pmcmc.Handle(0)
+    fleet = pmcmc.fleet_solve(chains, workers=4, handle=h)
+    assert any(m.dim > 256 for m, *_ in chains)  # both logistic contraction paths
+    for (model, sampler, x0, seed, block), (S, info, lp, acc) in zip(chains, fleet):
+        S1, i1, lp1, acc1 = pmcmc.solve(model, sampler, x0, seed=seed, block=block, handle=h,
+                                        return_logp=True)
+        assert info["converged"] == i1["converged"]
+        assert info["iters"] == i1["iters"]
+        assert np.array_equal(acc, acc1)
+        np.testing.assert_allclose(S, S1, rtol=1e-6, atol=1e-6)
+
+
+def test_fleet_reports_a_failing_chain():
+    chains = configs.logistic_fleet(n_chains=2, scale=0.05)
+    model, sampler, x0, seed, block = chains[1]
+    bad = pmcmc.ParallelMALASampler(sampler.epsilon, T=sampler.T, probes=1, dtype=np.float32)
+    bad.damping = 0.0  # invalid: ArgumentError from the library, not from the dataclass
+    chains[1] = (model, bad, x0, seed, block)
+    with pytest.raises(pmcmc.ArgumentError):
+        pmcmc.fleet_solve(chains, workers=2)
