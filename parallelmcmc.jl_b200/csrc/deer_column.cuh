@@ -186,10 +186,28 @@ struct Col {
 // at y, and the FP64 log acceptance ratio.  The D/2 log(4 pi eps) constants of
 // the two logq terms cancel exactly and are not formed; y - x - eps g_x is
 // sqrt(2 eps) xi by construction of y.
+// xi_pre: the column's tape normals already in registers (prefetched by the
+// caller), or nullptr to load them here.
+template <typename Real, int QPL>
+__device__ __forceinline__ void load_xi(const DevParams& P, int64_t t, float (&n)[QPL][4]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < P.D) {
+      load4(P.xi + t * P.Dp + 4 * j, n[q]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) n[q][e] = 0.f;
+    }
+  }
+}
+
 template <typename Real, int TK, int QPL>
 __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Real>& sm,
                                                const TapeKey& key, const Real* xcol, int t,
-                                               Col<Real, QPL>& c) {
+                                               Col<Real, QPL>& c,
+                                               const float (*xi_pre)[4] = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
   const Real eps = static_cast<Real>(P.eps), c2 = static_cast<Real>(P.sqrt2eps);
@@ -200,7 +218,12 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     if (4 * j < D) {
       load4(xcol + 4 * j, c.x[q]);
       float n[4];
-      load4(P.xi + static_cast<size_t>(t) * Dp + 4 * j, n);
+      if (xi_pre) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) n[e] = xi_pre[q][e];
+      } else {
+        load4(P.xi + static_cast<size_t>(t) * Dp + 4 * j, n);
+      }
 #pragma unroll
       for (int e = 0; e < 4; ++e) c.xi[q][e] = static_cast<Real>(n[e]);
     } else {

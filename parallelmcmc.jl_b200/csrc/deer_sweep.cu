@@ -221,29 +221,51 @@ __global__ void __launch_bounds__(kThreads)
 
   if (ncols > 0) {
     // ---- stage S_old columns t0-1 .. t0+ncols-1 ----
-    const int nstage = (ncols + 1) * Dp;
+    // quads, several loads in flight per thread
+    const int nq = Dp / 4;
+    const int nstage = (ncols + 1) * nq;
+#pragma unroll 4
     for (int i = tid; i < nstage; i += kThreads) {
-      const int c = i / Dp;
+      const int c = i / nq, k = 4 * (i - c * nq);
       const int64_t t = t0 - 1 + c;
-      Real v;
-      if (from_x0 || t < 0) v = x0[i - c * Dp];
-      else if (t < t_lo) v = Sold[(t_lo - 1) * Dp + (i - c * Dp)];  // s_{t_lo - 1}
-      else v = Sold[t * Dp + (i - c * Dp)];
-      sm.Xs[i] = v;
+      const Real* src = (from_x0 || t < 0) ? x0 + k
+                        : t < t_lo        ? Sold + (t_lo - 1) * Dp + k  // s_{t_lo - 1}
+                                          : Sold + t * Dp + k;
+      Real v[4];
+      load4(src, v);
+      store4(sm.Xs + c * Dp + k, v);
     }
     __syncthreads();
 
     // ---- phase 1: evaluate columns (one warp per column) ----
+    // The tape of the warp's next column is loaded while this one is computed.
     const TapeKey key(P.seed, P.block);
+    float xin[QPL][4];
+    double lun = 0.0;
+    if constexpr (TK != kLogistic) {
+      if (warp < ncols) {
+        load_xi<Real, QPL>(P, t0 + warp, xin);
+        lun = P.logu[t0 + warp];
+      }
+    }
     for (int c = warp; c < ncols; c += kWarps) {
       const int t = static_cast<int>(t0 + c);
       Real A[QPL][4], Bq[QPL][4];
       if constexpr (TK == kLogistic) {
         column_logistic<Real, QPL>(P, key, sm.Xs + c * Dp, t, iter, A, Bq);
       } else {
+        float xic[QPL][4];
+#pragma unroll
+        for (int q = 0; q < QPL; ++q)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) xic[q][e] = xin[q][e];
+        const double logu = lun;
+        if (c + kWarps < ncols) {
+          load_xi<Real, QPL>(P, t + kWarps, xin);
+          lun = P.logu[t + kWarps];
+        }
         Col<Real, QPL> col;
-        column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col);
-        const double logu = P.logu[t];
+        column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
         const bool acc = logu < col.la;
         const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
         const Real gp = static_cast<Real>(gd * (1.0 - gd));
@@ -412,14 +434,9 @@ __global__ void __launch_bounds__(kThreads)
     if (s_err) atomicExch(&st->status, static_cast<int>(kStTimeout));
     if (s_nonfinite) atomicCAS(&st->status, 0, static_cast<int>(kStNonfinite));
     __threadfence();
-    if constexpr (!COOP) {
-      const unsigned prev = atomicAdd(&st->done_counter, 1u);
-      s_last = (prev == gridDim.x - 1);
-    }
-  }
-  if constexpr (COOP) {
-    cg::this_grid().sync();
-    if (tid == 0) s_last = blockIdx.x == 0;
+    // the last CTA to arrive runs the convergence test (no third grid barrier)
+    const unsigned prev = atomicAdd(&st->done_counter, 1u);
+    s_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
   if (!s_last) return;
