@@ -12,7 +12,8 @@ The path does not shard (one chain), so N GPUs run N independent replicas
 
 Printed JSON: value = device-timed samples/s with inputs resident in HBM (L2
 flushed between steps), e2e = the same through pmcmc.sample() with host
-buffers, plain_gpu = the unfused reference-structured GPU path, roofline of
+buffers (one call of 8 blocks per step, wall clock; e2e.one_block: one block
+per call), plain_gpu = the unfused reference-structured GPU path, roofline of
 the sweep kernel, cpu_baseline = the FP64 CPU restatement of the reference
 algorithm on this host's cores.
 
@@ -37,6 +38,7 @@ sys.path.insert(0, os.path.join(ROOT, "parallelmcmc.jl_b200"))
 
 METRIC = "DEER samples/sec, batched+mixed vs plain GPU DEER, at trace err ≤1e-5 vs FP64"
 WORKLOAD = "diag_gauss_D100_T16384_diag_f32"
+E2E_BLOCKS = 8  # blocks of T samples per end-to-end sample() call
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 L2_FLUSH_BYTES = 512 << 20
 
@@ -232,7 +234,9 @@ def run_ours(args):
         total_ms = float(t.item())
     value = world * args.steps * T / (total_ms / 1e3)
     iters = [i.iters for i in infos]
-    launches = sum(2 + i.iters for i in infos)  # init + sweeps + finalize per block
+    persistent = bool(infos[0].path & 32)
+    # one cooperative launch per block (persistent solve), else init + sweeps + finalize
+    launches = sum(1 if persistent else 2 + i.iters for i in infos)
 
     # ---- parity of the timed workload: first timed block vs the FP64 sequential oracle
     parity = {}
@@ -269,29 +273,51 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     prof = h.profile(reset=True)
     h.set_profiling(False)
-    sweep_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
-    alg_bytes = 12 * D * T + 8 * T  # per sweep launch (S read, Xi read, S write, u read, logp write)
-    min_bytes = 8 * D * T + 4 * T  # what this kernel must move (tape regenerated in registers)
+    sweep_bytes = 12 * D * T + 8 * T  # one Newton sweep (S read, Xi read, S write, u read, logp write)
     hbm, src = peaks()
-    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
-    # dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of this workload,
-    # from the ncu capture summarised in profiles/deer_sweep_kernel_aniso_diag_d100.md
-    traffic = 6754048
+    if prof["solve_launches"]:
+        # persistent kernel: one launch = tape + every sweep + verification of a block
+        kernel = "deer_persist_kernel"
+        launch_ms = prof["solve_ms"] / prof["solve_launches"]
+        sweeps = prof["solve_sweeps"] / prof["solve_launches"]
+        alg_bytes = sweeps * sweep_bytes
+        min_bytes = 4 * D * T + 5 * T  # S, logp, accept out; S and the tape stay on chip
+        nprof = prof["solve_launches"]
+        traffic = None
+    else:
+        kernel = "deer_sweep_kernel"
+        launch_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
+        sweeps = 1.0
+        alg_bytes = sweep_bytes
+        min_bytes = 8 * D * T + 4 * T  # what this kernel must move (tape regenerated in registers)
+        nprof = prof["sweep_launches"]
+        # dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of this workload,
+        # from the ncu capture summarised in profiles/deer_sweep_kernel_aniso_diag_d100.md
+        traffic = 6754048
+    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
 
-    # ---- end to end through the public API with host buffers
-    x0_host = np.asarray(x0, np.float32)
-    pmcmc.sample(model, sampler, T, seed=seed, initial_params=x0_host, handle=h)
-    e2e_t = []
-    for k in range(max(3, args.steps // 2)):
-        t0 = time.perf_counter()
-        pmcmc.sample(model, sampler, T, seed=seed + 1 + k, initial_params=x0_host, handle=h)
-        e2e_t.append(time.perf_counter() - t0)
-    e2e_local = len(e2e_t) * T / sum(e2e_t)
-    e2e_val = e2e_local
-    if pg:
-        t = torch.tensor([sum(e2e_t)], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_val = world * len(e2e_t) * T / float(t.item())
+    # ---- end to end through the public API with host buffers: one sample() call of
+    # E2E_BLOCKS blocks per step (x0 in, the chain's values, logp and accept flags out;
+    # block b's copy-out overlaps block b + 1's solve), and of one block for reference
+    x0_host = torch.tensor(np.asarray(x0, np.float32)).pin_memory().numpy()
+
+    def e2e(nblocks, nsteps):
+        pmcmc.sample(model, sampler, nblocks * T, seed=seed, initial_params=x0_host, handle=h)
+        ts = []
+        for k in range(nsteps):
+            t0 = time.perf_counter()
+            pmcmc.sample(model, sampler, nblocks * T, seed=seed + 1 + k, initial_params=x0_host,
+                         handle=h)
+            ts.append(time.perf_counter() - t0)
+        total = sum(ts)
+        if pg:
+            t = torch.tensor([total], device=dev, dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            total = float(t.item())
+        return world * nsteps * nblocks * T / total
+
+    e2e_val = e2e(E2E_BLOCKS, max(3, args.steps // 2))
+    e2e_one = e2e(1, max(3, args.steps // 2))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -313,18 +339,24 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "D": D, "T": T, "eps": 0.05, "jacobian": "diag",
                        "state": "f32", "logalpha": "f64", "l2": "flushed (512 MB write) "
                        "between timed steps", "parallelism": f"replicas x{world}",
-                       "newton_iters_mean": statistics.mean(iters)},
+                       "newton_iters_mean": statistics.mean(iters),
+                       "path": [n for b, n in L.PATH_BITS if infos[0].path & b]},
             "e2e": {"value": e2e_val, "unit": "samples/s", "h2d_bytes_per_step": 4 * D,
-                    "d2h_bytes_per_step": 4 * D * T + 4 * T + T},
+                    "d2h_bytes_per_step": E2E_BLOCKS * (4 * D * T + 4 * T + T),
+                    "step": f"pmcmc.sample(N={E2E_BLOCKS}*T) from pinned x0 into pinned host "
+                            f"arrays, wall clock",
+                    "one_block": {"value": e2e_one, "step": "pmcmc.sample(N=T)",
+                                  "d2h_bytes_per_step": 4 * D * T + 4 * T + T}},
             "plain_gpu": {"value": plain_value, "unit": "samples/s",
                           "newton_iters_mean": statistics.mean(i.iters for i in pinfos),
                           "speedup_fused_over_plain": value / world / plain_value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
-                         "kernel": "deer_sweep_kernel", "avg_launch_ms": sweep_ms,
+                         "kernel": kernel, "avg_launch_ms": launch_ms,
+                         "sweeps_per_launch": sweeps,
                          "alg_bytes_per_launch": alg_bytes,
                          "kernel_min_bytes_per_launch": min_bytes,
-                         "launches_profiled": prof["sweep_launches"]},
+                         "launches_profiled": nprof},
             "cpu_baseline": cpu,
             "parity": parity,
             "gpu_launches": launches,

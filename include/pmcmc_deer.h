@@ -100,6 +100,7 @@ typedef struct {
 #define PMCMC_PATH_GRAPH 4        /* Newton loop in a CUDA graph while-node */
 #define PMCMC_PATH_TENSOR_CORE 8  /* logistic passes on tcgen05 tensor cores */
 #define PMCMC_PATH_FULL_JACOBIAN 16 /* :full mode (dense Jacobian, eigenbasis chunk scan) */
+#define PMCMC_PATH_PERSISTENT 32  /* whole solve in one cooperative launch, state in shared memory */
 
 /* ---- handle ------------------------------------------------------------ */
 /* Replaces DEERWorkspace (src/DEER/DEER.jl:47-90): owns all device workspace,
@@ -276,9 +277,23 @@ typedef struct {
   double finalize_ms;
   int64_t pass_launches;
   double pass_ms;       /* logistic target: one gradient/HVP contraction pass */
+  int64_t solve_launches;
+  double solve_ms;      /* persistent kernel: a whole solve (tape, sweeps, verification) */
+  int64_t solve_sweeps; /* Newton sweeps inside those launches */
 } pmcmc_profile;
 int pmcmc_set_profiling(pmcmc_handle* h, int32_t on);
 int pmcmc_get_profile(pmcmc_handle* h, pmcmc_profile* out, int32_t reset);
+
+/* ---- bound check of the device waits (no counterpart in the reference, whose
+ * device code never waits on another block) ------------------------------------
+ * Runs one of the library's bounded waits on a flag that nothing sets: the
+ * look-back spin of the scans and sweeps (PMCMC_WAIT_LOOKBACK), or the
+ * mbarrier wait of the tensor-core pass (PMCMC_WAIT_MBARRIER).  The wait
+ * gives up at its bound, the kernel returns normally and the call returns
+ * PMCMC_ERR_TIMEOUT with the device time in *wait_ms; the handle and its
+ * context stay usable.  PMCMC_OK would mean the wait ended without its flag. */
+typedef enum { PMCMC_WAIT_LOOKBACK = 0, PMCMC_WAIT_MBARRIER = 1 } pmcmc_wait_kind;
+int pmcmc_check_wait_bound(pmcmc_handle* h, int32_t kind, double* wait_ms);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,7 @@ struct pmcmc_handle {
   GraphKey gkey;
   bool force_eager = false;
   bool no_coop = false;
+  bool no_persist = false;  // solves of Gaussian targets through the per-sweep graph instead
   int tile_override = 0;
   unsigned long long* h_red = nullptr;  // pinned, plain-path metric readback
   cublasHandle_t cublas = nullptr;
@@ -84,6 +85,13 @@ struct pmcmc_handle {
   int full_chunks_override = 0;
   SliceState slice;
   std::vector<pmcmc_handle*> fleet;  // worker handles of pmcmc_fleet_solve (own streams)
+  // host-output pipeline of multi-block solves: block b's device-to-host copy
+  // runs on copy_stream while block b + 1 solves on stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_fin[2] = {nullptr, nullptr};   // block output ready (slot b & 1)
+  cudaEvent_t ev_copy[2] = {nullptr, nullptr};  // slot b & 1 copied out, reusable
+  DevState* h_states = nullptr;                 // pinned, one per block
+  int64_t h_states_cap = 0;
 };
 
 struct pmcmc_target {
@@ -166,6 +174,32 @@ int ensure_ws(pmcmc_handle* h, size_t bytes) {
   return PMCMC_OK;
 }
 
+// Copy stream, slot events and a pinned per-block state ring for a host-output
+// solve of nblocks blocks.
+int ensure_pipeline(pmcmc_handle* h, int64_t nblocks) {
+  if (!h->copy_stream) {
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&h->copy_stream, cudaStreamNonBlocking, lo));
+    for (int i = 0; i < 2; ++i) {
+      CK(cudaEventCreateWithFlags(&h->ev_fin[i], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h->ev_copy[i], cudaEventDisableTiming));
+    }
+  }
+  if (nblocks > h->h_states_cap) {
+    if (h->h_states) {
+      CK(cudaStreamSynchronize(h->stream));
+      CK(cudaFreeHost(h->h_states));
+      h->h_states = nullptr;
+      h->h_states_cap = 0;
+    }
+    const int64_t cap = std::max<int64_t>(nblocks, 64);
+    CK(cudaMallocHost(&h->h_states, sizeof(DevState) * static_cast<size_t>(cap)));
+    h->h_states_cap = cap;
+  }
+  return PMCMC_OK;
+}
+
 // Reference argument validation (DEER.jl:387-393, 525-528; interface.jl:273-275).
 int validate(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p) {
   if (!p) return fail(h, PMCMC_ERR_ARGUMENT, "params must not be NULL");
@@ -238,6 +272,28 @@ TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t D
   return tp;
 }
 
+// Columns per CTA of the persistent solve: the smallest power of two whose
+// tiles are all co-resident (one cooperative launch); 0 when none is.
+int choose_persist_tile(pmcmc_handle* h, const void* fn, bool f64, int64_t Dp, int64_t T,
+                        bool dense) {
+  if (!fn || h->no_coop || h->tile_override > 0) return 0;
+  for (int TT = 8; TT <= 256; TT <<= 1) {
+    const size_t smem = persist_smem(f64, Dp, TT, dense).total;
+    if (smem > 200 * 1024) break;
+    if (raise_smem_limit(fn, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    if (nb > 0 && (T + TT - 1) / TT <= static_cast<int64_t>(nb) * h->num_sms) return TT;
+  }
+  return 0;
+}
+
 cudaError_t launch_sweep(const void* fn, bool coop, int grid, size_t smem, void** args,
                          cudaStream_t s) {
   if (coop)
@@ -254,12 +310,14 @@ struct SolveLayout {
   size_t tcws, Gtc;  // tensor-core logistic path
   size_t fU, fV, fR, facc, fPhi, fbeta, fdin, eS0, eS1, exi, ex0;  // :full mode
   size_t alam, acterm, aarev, adirect, ascr, aout;                 // adjoint
+  size_t out2_S, out2_lp, out2_acc;  // second output slot of the host-output pipeline
   size_t total;
 };
 
 SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain,
                    int64_t N = 0, int64_t Tc = 0, size_t tc_bytes = 0,
-                   const FullPlan* fp = nullptr, bool adjoint = false) {
+                   const FullPlan* fp = nullptr, bool adjoint = false,
+                   bool dual_out = false) {
   SolveLayout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -274,11 +332,16 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
   L.flags = take(4 * static_cast<size_t>(ntiles));
   L.agg_a = take(es * ntiles * Dp);
   L.agg_b = take(es * ntiles * Dp);
-  L.incl = take(es * ntiles * Dp);
+  L.incl = take(es * (ntiles + 1) * Dp);  // + the persistent solve's S_0
   L.colmax = take(4 * static_cast<size_t>(T));
   L.out_S = take(es * T * D);
   L.out_lp = take(es * T);
   L.out_acc = take(static_cast<size_t>(T));
+  if (dual_out) {
+    L.out2_S = take(es * T * D);
+    L.out2_lp = take(es * T);
+    L.out2_acc = take(static_cast<size_t>(T));
+  }
   L.xi = take(4 * T * Dp);
   L.logu = take(8 * static_cast<size_t>(T));
   if (plain) {
@@ -466,6 +529,29 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
     CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
     h->prof.finalize_launches += 1;
     h->prof.finalize_ms += ms;
+  }
+  return PMCMC_OK;
+}
+
+// One DEER block as one cooperative launch of the persistent solve kernel
+// (tape, every sweep and the verification pass; deer_persist.cu).
+int run_persist(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t smem) {
+  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
+  CK(raise_smem_limit(k.persist, smem));
+  void* args[] = {&h->d_params, &h->d_state};
+  if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
+  CK(cudaLaunchCooperativeKernel(k.persist, dim3(P.ntiles), dim3(kThreads), args, smem,
+                                 h->stream));
+  if (h->profiling) {
+    CK(cudaEventRecord(h->ev[1], h->stream));
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+    h->prof.solve_launches += 1;
+    h->prof.solve_ms += ms;
+    h->prof.solve_sweeps += h->h_state->iter;
   }
   return PMCMC_OK;
 }
@@ -1007,7 +1093,14 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   }
   const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
                                   : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
-  const TilePlan tp = full ? TilePlan{} : choose_tile(h, k, f64, Dp, W, dense);
+  // whole solve in one cooperative launch when every tile is co-resident
+  const int TTp = (!plain && !logistic && !full && W == T && !h->force_eager && !h->no_persist)
+                      ? choose_persist_tile(h, k.persist, f64, Dp, T, dense)
+                      : 0;
+  const bool persist = TTp > 0;
+  const TilePlan tp = full      ? TilePlan{}
+                      : persist ? TilePlan{TTp, true}
+                                : choose_tile(h, k, f64, Dp, W, dense);
   const int TT = tp.TT;
   const int ntiles = static_cast<int>((W + TT - 1) / TT);
   const SmemPlan sp_sweep = gauss_sweep_smem(f64, Dp, TT, dense);
@@ -1017,10 +1110,25 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
                 (long long)D);
   const bool use_tc = logistic && !plain && !f64 && lg_tc_supported(tg->lg);
   const int64_t Tc = logistic && !use_tc ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
+  const int64_t nblocks = (N + T - 1) / T;
+  // Host outputs of several blocks: block b's copy-out overlaps block b + 1's solve.
+  const bool pipe = mem == PMCMC_MEM_HOST && nblocks > 1;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
-                               use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr);
+                               use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr,
+                               false, pipe);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
+  if (pipe) {
+    rc = ensure_pipeline(h, nblocks);
+    if (rc) return rc;
+  }
+  // copies still in flight into the caller's buffers end before any return
+  struct CopyDrain {
+    cudaStream_t s;
+    ~CopyDrain() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } drain{pipe ? h->copy_stream : nullptr};
   unsigned char* ws = h->ws;
 
   // x0 -> padded device buffer
@@ -1097,11 +1205,13 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
                                                           int64_t(h->num_sms) * 8));
   const int init_grid = static_cast<int>(
       std::min<int64_t>((T * (Dp / 4) + 255) / 256, int64_t(h->num_sms) * 8));
-  const int64_t nblocks = (N + T - 1) / T;
   std::vector<DevState> states(static_cast<size_t>(nblocks));
   int64_t nsteps = 0;
   for (int64_t b = 0; b < nblocks; ++b) {
     const int64_t nkeep = std::min<int64_t>(T, N - nsteps);
+    const bool slot = pipe && (b & 1);
+    const size_t oS = slot ? L.out2_S : L.out_S, olp = slot ? L.out2_lp : L.out_lp,
+                 oacc = slot ? L.out2_acc : L.out_acc;
     P.block = block0 + static_cast<uint64_t>(b);
     P.x0 = ws + ((b & 1) ? L.x0b : L.x0a);
     P.x_next = ws + ((b & 1) ? L.x0a : L.x0b);
@@ -1111,34 +1221,59 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       P.logp_out = logp_out ? static_cast<unsigned char*>(logp_out) + es * nsteps : nullptr;
       P.accept_out = accept_out ? accept_out + nsteps : nullptr;
     } else {
-      P.S_out = ws + L.out_S;
-      P.logp_out = logp_out ? ws + L.out_lp : nullptr;
-      P.accept_out = accept_out ? ws + L.out_acc : nullptr;
+      P.S_out = ws + oS;
+      P.logp_out = logp_out ? ws + olp : nullptr;
+      P.accept_out = accept_out ? ws + oacc : nullptr;
     }
+    // the slot's previous contents (block b - 2) must be copied out first
+    if (pipe && b >= 2) CK(cudaStreamWaitEvent(h->stream, h->ev_copy[slot], 0));
     rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid,
                                  init_grid, Tc, use_tc)
          : full   ? run_full(h, k, fplan, P, eigen_view(P, tg, ws, L), F, sp_fin.total,
                              fin_grid, init_grid)
-         : plain  ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
-                  : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
-                              init_grid);
+         : plain   ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
+         : persist ? run_persist(h, k, P, persist_smem(f64, Dp, TT, dense).total)
+                   : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
+                               init_grid);
     if (rc) return rc;
     if (mem == PMCMC_MEM_HOST) {
-      CK(cudaMemcpyAsync(static_cast<unsigned char*>(S_out) + es * nsteps * D, ws + L.out_S,
-                         es * nkeep * D, cudaMemcpyDeviceToHost, h->stream));
+      cudaStream_t cs = h->stream;
+      if (pipe) {
+        CK(cudaEventRecord(h->ev_fin[slot], h->stream));
+        CK(cudaStreamWaitEvent(h->copy_stream, h->ev_fin[slot], 0));
+        cs = h->copy_stream;
+      }
+      CK(cudaMemcpyAsync(static_cast<unsigned char*>(S_out) + es * nsteps * D, ws + oS,
+                         es * nkeep * D, cudaMemcpyDeviceToHost, cs));
       if (logp_out)
-        CK(cudaMemcpyAsync(static_cast<unsigned char*>(logp_out) + es * nsteps, ws + L.out_lp,
-                           es * nkeep, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(static_cast<unsigned char*>(logp_out) + es * nsteps, ws + olp,
+                           es * nkeep, cudaMemcpyDeviceToHost, cs));
       if (accept_out)
-        CK(cudaMemcpyAsync(accept_out + nsteps, ws + L.out_acc, nkeep, cudaMemcpyDeviceToHost,
-                           h->stream));
+        CK(cudaMemcpyAsync(accept_out + nsteps, ws + oacc, nkeep, cudaMemcpyDeviceToHost, cs));
+      if (pipe) CK(cudaEventRecord(h->ev_copy[slot], cs));
+    }
+    nsteps += nkeep;
+    if (pipe) {  // block states are read after the last block
+      CK(cudaMemcpyAsync(h->h_states + b, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                         h->stream));
+      continue;
     }
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     states[static_cast<size_t>(b)] = *h->h_state;
-    nsteps += nkeep;
     if (h->h_state->status) break;
+  }
+  if (pipe) {
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaStreamSynchronize(h->copy_stream));
+    for (int64_t b = 0; b < nblocks; ++b) {
+      states[static_cast<size_t>(b)] = h->h_states[b];
+      if (h->h_states[b].status) {  // the blocks after a failed one do not count
+        states.resize(static_cast<size_t>(b + 1));
+        break;
+      }
+    }
   }
   // aggregate
   pmcmc_info agg{};
@@ -1160,7 +1295,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (nblocks == 1) fill_info(states[0], &agg);
   agg.path = (plain || full ? 0 : PMCMC_PATH_FUSED_SWEEP) |
              (tp.coop && !plain && !full ? PMCMC_PATH_COOPERATIVE : 0) |
-             (!plain && !logistic && !h->force_eager && !h->profiling ? PMCMC_PATH_GRAPH : 0) |
+             (!plain && !logistic && !persist && !h->force_eager && !h->profiling
+                  ? PMCMC_PATH_GRAPH
+                  : 0) |
+             (persist ? PMCMC_PATH_PERSISTENT : 0) |
              (use_tc ? PMCMC_PATH_TENSOR_CORE : 0) | (full ? PMCMC_PATH_FULL_JACOBIAN : 0);
   if (info) *info = agg;
   return status_error(h, status);
@@ -1260,6 +1398,8 @@ int pmcmc_create(int device, void* stream, pmcmc_handle** out) {
   h->force_eager = ev && ev[0] == '1';
   const char* cv = std::getenv("PMCMC_NO_COOP");
   h->no_coop = cv && cv[0] == '1';
+  const char* nv = std::getenv("PMCMC_NO_PERSIST");
+  h->no_persist = nv && nv[0] == '1';
   const char* tv = std::getenv("PMCMC_TILE_COLS");
   h->tile_override = tv ? std::atoi(tv) : 0;
   const char* fv = std::getenv("PMCMC_FULL_CHUNKS");
@@ -1289,6 +1429,15 @@ int pmcmc_destroy(pmcmc_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->gexec_full) cudaGraphExecDestroy(h->gexec_full);
   for (pmcmc_handle* w : h->fleet) pmcmc_destroy(w);
+  if (h->copy_stream) {
+    cudaStreamSynchronize(h->copy_stream);
+    cudaStreamDestroy(h->copy_stream);
+  }
+  for (int i = 0; i < 2; ++i) {
+    if (h->ev_fin[i]) cudaEventDestroy(h->ev_fin[i]);
+    if (h->ev_copy[i]) cudaEventDestroy(h->ev_copy[i]);
+  }
+  if (h->h_states) cudaFreeHost(h->h_states);
   if (h->cublas) cublasDestroy(h->cublas);
   cudaFree(h->d_full);
   cudaFree(h->d_params_e);
@@ -1323,6 +1472,43 @@ int pmcmc_get_profile(pmcmc_handle* h, pmcmc_profile* out, int32_t reset) {
   *out = h->prof;
   if (reset) h->prof = pmcmc_profile{};
   return PMCMC_OK;
+}
+
+int pmcmc_check_wait_bound(pmcmc_handle* h, int32_t kind, double* wait_ms) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  if (kind != PMCMC_WAIT_LOOKBACK && kind != PMCMC_WAIT_MBARRIER)
+    return fail(h, PMCMC_ERR_ARGUMENT, "kind must be PMCMC_WAIT_LOOKBACK or PMCMC_WAIT_MBARRIER");
+  DeviceGuard guard(h->device);
+  struct Scratch {
+    void* buf = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Scratch() {
+      cudaFree(buf);  // synchronises the device first
+      for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    }
+  } sc;
+  CK(cudaMalloc(&sc.buf, 256));
+  CK(cudaEventCreate(&sc.ev[0]));
+  CK(cudaEventCreate(&sc.ev[1]));
+  uint32_t* flags = static_cast<uint32_t*>(sc.buf);                    // 32 zero words
+  int* err = reinterpret_cast<int*>(static_cast<char*>(sc.buf) + 128);  // out
+  CK(cudaMemsetAsync(sc.buf, 0, 256, h->stream));
+  CK(cudaEventRecord(sc.ev[0], h->stream));
+  if (kind == PMCMC_WAIT_LOOKBACK)
+    CK(launch_lookback_bound(h->stream, flags, err));
+  else
+    CK(lg_tc_mbar_bound(h->stream, err));
+  CK(cudaEventRecord(sc.ev[1], h->stream));
+  int gave_up = 0;
+  CK(cudaMemcpyAsync(&gave_up, err, sizeof gave_up, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, sc.ev[0], sc.ev[1]));
+  if (wait_ms) *wait_ms = ms;
+  if (!gave_up) return PMCMC_OK;
+  return fail(h, PMCMC_ERR_TIMEOUT, "%s wait reached its bound after %.1f ms",
+              kind == PMCMC_WAIT_LOOKBACK ? "look-back" : "mbarrier", ms);
 }
 
 int pmcmc_target_diag_gauss(pmcmc_handle* h, int64_t D, const double* mean, const double* prec,

@@ -228,4 +228,50 @@ __device__ __forceinline__ Real lookback_compose(int tile, int jstar, int d, int
   return a * __ldcg(incl + static_cast<size_t>(jstar) * Dp + d) + b;
 }
 
+// Cooperative sweep, phase B: for coordinate d, the state entering every tile
+// (exclusive scan of the tile aggregates in tile order, applied to s_lo) by
+// one CTA: each thread composes a run of consecutive tiles, a Kogge-Stone scan
+// over the 256 run aggregates in shared memory, then each run is replayed.
+template <typename Real>
+__device__ void carry_scan_tiles(int ntiles, int d, int Dp, const Real* __restrict__ agg_a,
+                                 const Real* __restrict__ agg_b, Real s_lo,
+                                 Real* __restrict__ carry, Real* sa, Real* sb) {
+  const int tid = threadIdx.x;
+  const int K = (ntiles + kThreads - 1) / kThreads;
+  const int j0 = min(ntiles, tid * K), j1 = min(ntiles, j0 + K);
+  Real a = 1, b = 0;
+  for (int j = j0; j < j1; ++j) {
+    const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
+    const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
+    b = aj * b + bj;
+    a = aj * a;
+  }
+  sa[tid] = a;
+  sb[tid] = b;
+  __syncthreads();
+  for (int off = 1; off < kThreads; off <<= 1) {
+    Real pa = 1, pb = 0;
+    if (tid >= off) {
+      pa = sa[tid - off];
+      pb = sb[tid - off];
+    }
+    __syncthreads();
+    if (tid >= off) {
+      const Real ma = sa[tid], mb = sb[tid];
+      sa[tid] = ma * pa;
+      sb[tid] = ma * pb + mb;
+    }
+    __syncthreads();
+  }
+  Real st = s_lo;
+  if (tid > 0) st = sa[tid - 1] * s_lo + sb[tid - 1];
+  for (int j = j0; j < j1; ++j) {
+    carry[static_cast<size_t>(j) * Dp + d] = st;
+    const Real aj = __ldcg(agg_a + static_cast<size_t>(j) * Dp + d);
+    const Real bj = __ldcg(agg_b + static_cast<size_t>(j) * Dp + d);
+    st = aj * st + bj;
+  }
+  __syncthreads();
+}
+
 }  // namespace pmcmc

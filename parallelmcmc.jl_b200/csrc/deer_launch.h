@@ -18,8 +18,18 @@ struct SweepKernels {
   const void* finalize = nullptr;  // (const DevParams*, DevState*)
   const void* init = nullptr;      // (const DevParams*, DevState*)
   const void* eval = nullptr;      // (const DevParams*, const Real* Sold, int iter, int from_x0, Real* A, Real* B)
+  const void* persist = nullptr;   // (const DevParams*, DevState*): whole solve, cooperative
   int qpl = 1;
 };
+
+// Shared memory of the persistent solve kernel (deer_persist.cu): the sweep
+// plan at TT columns plus the CTA's tape (TT + 1 columns of xi and log u).
+struct PersistPlan {
+  SmemPlan sweep;
+  size_t xi, lu, total;
+};
+PersistPlan persist_smem(bool f64, int64_t Dp, int TT, bool dense);
+const void* persist_kernel(bool f64, int tk, int jac, int qpl);
 
 // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never
 // lowering it: the attribute is global per function, and handles on other
@@ -58,6 +68,10 @@ cudaError_t launch_doubling_scan(cudaStream_t s, bool f64, int64_t Dp, int64_t T
 cudaError_t launch_damp_metric(cudaStream_t s, bool f64, int64_t D, int64_t Dp, int64_t T,
                                const void* S_old, void* S_new, double damping,
                                unsigned long long* red);
+
+// One look-back over `flags` (>= 1 zero word) that nothing publishes; err[0] =
+// 1 when the wait reached its bound (bound check of the scans' waits).
+cudaError_t launch_lookback_bound(cudaStream_t s, const uint32_t* flags, int* err);
 
 cudaError_t launch_broadcast(cudaStream_t s, bool f64, int64_t Dp, int64_t T, const void* x0,
                              void* S);

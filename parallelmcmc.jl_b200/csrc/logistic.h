@@ -42,5 +42,8 @@ size_t lg_tc_ws_bytes(const LogisticDev& X, int64_t T);
 int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const DevState* dS,
                double* lp, int mode, int64_t T, void* ws, float* G);
 int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T);
+// One bounded mbarrier wait that nothing completes (bound check); err[0] = 1
+// when it gave up.
+cudaError_t lg_tc_mbar_bound(cudaStream_t s, int* err);
 
 }  // namespace pmcmc

@@ -465,7 +465,23 @@ __global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
   }
 }
 
+// Bound check of the mbarrier wait used by the tensor-core pass: one thread
+// initialises a barrier that expects one arrival, nobody arrives, and the
+// bounded wait on phase 0 gives up after kWaitCycles; err[0] = 1 then.
+__global__ void mbar_bound_kernel(int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_err;
+  if (threadIdx.x == 0) {
+    s_err = 0;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) err[0] = mbar_wait(&bar, 0, &s_err) ? 0 : 1;
+}
+
 }  // namespace tc
+
 
 // ---------------------------------------------------------------------------
 // Host side
@@ -536,6 +552,11 @@ int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const 
   tc::logistic_pass_tc_kernel<<<grid, tc::kThreadsTC, Ly.total, s>>>(
       mXh, mXl, mBh, mBl, mBt, X.y32, X.N, nkb, T, X.Dp, G, lp, mode != 2 ? 1 : 0, err);
   return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+cudaError_t lg_tc_mbar_bound(cudaStream_t s, int* err) {
+  tc::mbar_bound_kernel<<<1, 32, 0, s>>>(err);
+  return cudaGetLastError();
 }
 
 }  // namespace pmcmc

@@ -309,4 +309,19 @@ cudaError_t launch_broadcast(cudaStream_t s, bool f64, int64_t Dp, int64_t T, co
   return cudaGetLastError();
 }
 
+// Bound check of the look-back wait: one warp looks back from tile 1 over a
+// flag array that nothing publishes (all zeros: no epoch, no state), so lane 0
+// spins until kMaxSpins and the warp reports the give-up in err[0].  The same
+// routine guards every scan and sweep launch.
+__global__ void lookback_bound_kernel(const uint32_t* flags, int* err) {
+  int e = 0;
+  lookback_window(1, 1u, flags, &e);
+  if (threadIdx.x == 0) err[0] = e;
+}
+
+cudaError_t launch_lookback_bound(cudaStream_t s, const uint32_t* flags, int* err) {
+  lookback_bound_kernel<<<1, 32, 0, s>>>(flags, err);
+  return cudaGetLastError();
+}
+
 }  // namespace pmcmc

@@ -27,9 +27,10 @@ SYMBOLS = [
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
     "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
-    "pmcmc_fleet_solve",
+    "pmcmc_fleet_solve", "pmcmc_check_wait_bound",
 ]
 OBJECTIVE = {"esjd": 0, "mean_sq": 1}
+WAIT_KIND = {"lookback": 0, "mbarrier": 1}
 
 
 class ArgumentError(ValueError):
@@ -60,7 +61,9 @@ class DeerParams(C.Structure):
 class Profile(C.Structure):
     _fields_ = [("sweep_launches", C.c_int64), ("sweep_ms", C.c_double),
                 ("finalize_launches", C.c_int64), ("finalize_ms", C.c_double),
-                ("pass_launches", C.c_int64), ("pass_ms", C.c_double)]
+                ("pass_launches", C.c_int64), ("pass_ms", C.c_double),
+                ("solve_launches", C.c_int64), ("solve_ms", C.c_double),
+                ("solve_sweeps", C.c_int64)]
 
 
 class Info(C.Structure):
@@ -84,7 +87,7 @@ class FleetChain(C.Structure):
 
 
 PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core"),
-             (16, "full_jacobian")]
+             (16, "full_jacobian"), (32, "persistent")]
 
 
 _vp = C.c_void_p
@@ -134,6 +137,7 @@ def load(path: str = LIB_PATH):
         L.pmcmc_slice_result.argtypes = [_vp, _vp, _vp, _vp, _vp, C.POINTER(Info), C.c_int32]
         L.pmcmc_deer_adjoint.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
                                          C.c_uint64, _vp, C.c_int32, C.c_int32, _vp]
+        L.pmcmc_check_wait_bound.argtypes = [_vp, C.c_int32, C.POINTER(C.c_double)]
         for fn in SYMBOLS:
             if fn not in ("pmcmc_last_error", "pmcmc_abi_version"):
                 getattr(L, fn).restype = C.c_int
@@ -179,6 +183,21 @@ class Handle:
         p = Profile()
         check(load().pmcmc_get_profile(self.ptr, C.byref(p), int(reset)), self.ptr, "profile")
         return {k: getattr(p, k) for k, _ in p._fields_}
+
+    def check_wait_bound(self, kind: str = "lookback") -> dict:
+        """Run one of the library's bounded device waits ("lookback" or
+        "mbarrier") on a flag that nothing sets.  A working bound returns
+        status ERR_TIMEOUT with the device time the wait took; the handle
+        stays usable afterwards."""
+        if kind not in WAIT_KIND:
+            raise ArgumentError(f"kind must be one of {sorted(WAIT_KIND)}")
+        L = load()
+        ms = C.c_double(0.0)
+        rc = L.pmcmc_check_wait_bound(self.ptr, WAIT_KIND[kind], C.byref(ms))
+        if rc not in (OK, ERR_TIMEOUT):
+            check(rc, self.ptr, "check_wait_bound")
+        m = L.pmcmc_last_error(self.ptr) if rc else b""
+        return {"status": rc, "wait_ms": ms.value, "message": m.decode() if m else ""}
 
     def close(self):
         if getattr(self, "ptr", None):

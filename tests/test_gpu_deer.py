@@ -258,12 +258,73 @@ def test_eager_loop_matches_graph(monkeypatch):
     monkeypatch.setenv("PMCMC_EAGER", "1")
     he = pmcmc.Handle(0)
     monkeypatch.delenv("PMCMC_EAGER")
+    monkeypatch.setenv("PMCMC_NO_PERSIST", "1")  # the per-sweep kernels in a graph
     hg = pmcmc.Handle(0)
     model, sampler, x0, meta = configs.quickstart_2d()
     Se, ie = pmcmc.solve(model, sampler, x0, seed=3, block=1, handle=he)
     Sg, ig = pmcmc.solve(model, sampler, x0, seed=3, block=1, handle=hg)
+    assert "graph" in ig["path_names"] and "persistent" not in ig["path_names"]
     assert ie["iters"] == ig["iters"]
     np.testing.assert_array_equal(Se, Sg)
+
+
+def _persist_cases():
+    """(name, model, sampler kwargs, x0, iteration slack, trace-error bar vs the
+    FP64 sequential chain).  The slack is 0 where the Newton iteration converges
+    fast; FP32 cases whose stopping rule sits near FP32 resolution (slow linear
+    convergence of a stochastic or diagonal Jacobian) stop a few sweeps apart
+    because rounding differs between the two scan associations."""
+    rng = np.random.default_rng(31)
+    lam = 10 ** rng.uniform(-1, 1, 100)
+    x100 = rng.standard_normal(100).astype(np.float32)
+    d64 = configs.correlated_gauss_d64(T=512, jacobian="diag")
+    return [
+        ("diag_f32", pmcmc.DensityModel.diag_gaussian(lam),
+         dict(T=2048, jacobian="diag", dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6), x100,
+         0, 1e-5),
+        ("stoch_f32_odd_T", pmcmc.DensityModel.diag_gaussian(lam),
+         dict(T=2047, jacobian="stoch_diag", dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6,
+              maxiter=1000), x100, 4, 1e-5),
+        # default stopping rule with damping 0.5: the last column stops ~tol from f(x)
+        ("diag_f64_D3_T1", pmcmc.DensityModel.diag_gaussian(np.ones(3)),
+         dict(T=1, jacobian="diag"), np.ones(3), 0, 1e-4),
+        ("stoch_f64_D5_T33", pmcmc.DensityModel.diag_gaussian(np.arange(1.0, 6.0)),
+         dict(T=33, jacobian="stoch_diag", probes=2, tol_abs=1e-10, tol_rel=1e-9), np.ones(5),
+         0, 1e-8),
+        ("dense_f32", d64[0], dict(T=512, jacobian="stoch_diag", dtype=np.float32,
+                                   tol_abs=1e-8, tol_rel=2e-7, maxiter=2000), d64[2], 25, 1e-5),
+    ]
+
+
+@pytest.mark.parametrize("case", range(5))
+def test_persistent_solve_matches_graph_path(monkeypatch, case):
+    """The whole-solve cooperative kernel and the per-sweep graph path run the
+    same Newton iteration (only the association of the cross-tile scan
+    differs): identical accept flags, iteration counts within the case's slack,
+    trajectories and logp equal to the stopping tolerance, and both verify
+    against the FP64 oracle."""
+    name, model, kw, x0, slack, bar = _persist_cases()[case]
+    hp = pmcmc.Handle(0)
+    monkeypatch.setenv("PMCMC_NO_PERSIST", "1")
+    hg = pmcmc.Handle(0)
+    sampler = pmcmc.ParallelMALASampler(0.05, **kw)
+    Sp, ip, lpp, ap = _run(hp, model, sampler, x0, 8, 2)
+    Sg, ig, lpg, ag = _run(hg, model, sampler, x0, 8, 2)
+    assert "persistent" in ip["path_names"], (name, ip["path_names"])
+    assert "persistent" not in ig["path_names"]
+    assert ip["converged"] == ig["converged"] == 1, (name, ip, ig)
+    assert abs(ip["iters"] - ig["iters"]) <= slack, (name, ip["iters"], ig["iters"])
+    assert np.array_equal(ap, ag), name
+    assert ip["n_accept"] == ig["n_accept"]
+    tol = 2e-5 if sampler.dtype == np.float32 else 1e-10
+    assert trace_err(Sp, Sg) <= tol, name
+    np.testing.assert_allclose(lpp, lpg, rtol=tol, atol=tol * np.abs(lpg).max())
+    tg = _oracle_target(model)
+    Xi, u = O.tape(8, 2, model.dim, sampler.T)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, 0.05, np.asarray(x0, np.float64), Xi, u)
+    assert np.array_equal(ap, acc_seq), name
+    assert trace_err(Sp, S_seq) <= bar, name
+    assert ip["max_defect"] <= 10 * bar * (1 + np.abs(Sp).max()), name
 
 
 def test_sample_quickstart_matches_fixture(h):
@@ -288,6 +349,25 @@ def test_sample_device_tensors_match_host(h):
     assert b.values.is_cuda
     np.testing.assert_array_equal(a.values, b.values.cpu().numpy())
     np.testing.assert_array_equal(a.logp, b.logp.cpu().numpy())
+
+
+def test_sample_host_pipeline_matches_device_output(h):
+    # host outputs of a multi-block sample are copied out while the next block
+    # solves (two output slots); the chain must equal the device-output chain,
+    # including a ragged last block, for several calls on one handle
+    torch = pytest.importorskip("torch")
+    prec = 10 ** np.random.default_rng(1).uniform(-2, 2, 100)
+    model = pmcmc.DensityModel.diag_gaussian(prec)
+    sampler = pmcmc.ParallelMALASampler(0.05, T=2048, jacobian="diag", dtype=np.float32)
+    x0 = np.random.default_rng(0).standard_normal(100).astype(np.float32)
+    for N, seed in ((5 * 2048 + 100, 4), (2 * 2048, 5), (3 * 2048 - 1, 6)):
+        a = pmcmc.sample(model, sampler, N, seed=seed, initial_params=x0, handle=h)
+        b = pmcmc.sample(model, sampler, N, seed=seed, initial_params=torch.from_numpy(x0).cuda(),
+                         handle=h)
+        np.testing.assert_array_equal(a.values, b.values.cpu().numpy())
+        np.testing.assert_array_equal(a.logp, b.logp.cpu().numpy())
+        np.testing.assert_array_equal(a.accepted, b.accepted.cpu().numpy())
+        assert a.info["iters"] == b.info["iters"] and a.info["converged"] == 1
 
 
 def test_step_api_walks_and_resolves(h):
