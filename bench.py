@@ -184,7 +184,11 @@ def run_ours(args):
         pg = dist
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # one explicit stream for the L2 flush, the CUDA events and the library, so that
+    # the events bracket the solve (torch's default stream is the legacy stream 0,
+    # which a handle would replace by a non-blocking stream of its own)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     h = pmcmc.Handle(local, stream=stream.cuda_stream)
     lib = L.load()
 
@@ -283,7 +287,9 @@ def run_ours(args):
         alg_bytes = sweeps * sweep_bytes
         min_bytes = 4 * D * T + 5 * T  # S, logp, accept out; S and the tape stay on chip
         nprof = prof["solve_launches"]
-        traffic = None
+        # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload,
+        # from the ncu capture summarised in profiles/deer_persist_kernel_aniso_diag_d100.md
+        traffic = 176896
     else:
         kernel = "deer_sweep_kernel"
         launch_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
@@ -382,7 +388,8 @@ def run_secondary(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # flush, events and library in one stream
+    torch.cuda.set_stream(stream)
     h = pmcmc.Handle(0, stream=stream.cuda_stream)
     lib = L.load()
     logistic = args.workload == "logistic_n10k_d256"

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -231,6 +232,31 @@ int validate(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p)
   return PMCMC_OK;
 }
 
+// Resident CTAs per SM of a kernel at kThreads threads and `smem` bytes of
+// dynamic shared memory, cached per (kernel, bytes): the query costs
+// microseconds of host time and a solve asks for several sizes.
+int max_active_blocks(const void* fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, size_t>, int> cache;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({fn, smem});
+    if (it != cache.end()) return it->second;
+  }
+  if (raise_smem_limit(fn, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  cache[{fn, smem}] = nb;
+  return nb;
+}
+
 struct TilePlan {
   int TT = 8;
   bool coop = false;
@@ -251,13 +277,8 @@ TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t D
     for (int TT = 8; TT <= 256; TT <<= 1) {
       const size_t smem = gauss_sweep_smem(f64, Dp, TT, dense).total;
       if (smem > 200 * 1024) break;
-      raise_smem_limit(reinterpret_cast<const void*>(k.sweep_coop), smem);
-      int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.sweep_coop, kThreads, smem) !=
-          cudaSuccess) {
-        cudaGetLastError();
-        break;
-      }
+      const int nb = max_active_blocks(k.sweep_coop, smem);
+      if (nb < 0) break;
       if (nb > 0 && (W + TT - 1) / TT <= static_cast<int64_t>(nb) * h->num_sms) {
         tp.TT = TT;
         tp.coop = true;
@@ -280,15 +301,8 @@ int choose_persist_tile(pmcmc_handle* h, const void* fn, bool f64, int64_t Dp, i
   for (int TT = 8; TT <= 256; TT <<= 1) {
     const size_t smem = persist_smem(f64, Dp, TT, dense).total;
     if (smem > 200 * 1024) break;
-    if (raise_smem_limit(fn, smem) != cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kThreads, smem) != cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
+    const int nb = max_active_blocks(fn, smem);
+    if (nb < 0) return 0;
     if (nb > 0 && (T + TT - 1) / TT <= static_cast<int64_t>(nb) * h->num_sms) return TT;
   }
   return 0;
@@ -311,6 +325,7 @@ struct SolveLayout {
   size_t fU, fV, fR, facc, fPhi, fbeta, fdin, eS0, eS1, exi, ex0;  // :full mode
   size_t alam, acterm, aarev, adirect, ascr, aout;                 // adjoint
   size_t out2_S, out2_lp, out2_acc;  // second output slot of the host-output pipeline
+  size_t part;                       // per-CTA partial reductions of the persistent solve
   size_t total;
 };
 
@@ -334,6 +349,7 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
   L.agg_b = take(es * ntiles * Dp);
   L.incl = take(es * (ntiles + 1) * Dp);  // + the persistent solve's S_0
   L.colmax = take(4 * static_cast<size_t>(T));
+  L.part = take(8 * 8 * static_cast<size_t>(ntiles));
   L.out_S = take(es * T * D);
   L.out_lp = take(es * T);
   L.out_acc = take(static_cast<size_t>(T));
@@ -536,9 +552,9 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
 // One DEER block as one cooperative launch of the persistent solve kernel
 // (tape, every sweep and the verification pass; deer_persist.cu).
 int run_persist(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t smem) {
-  CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   CK(raise_smem_limit(k.persist, smem));
-  void* args[] = {&h->d_params, &h->d_state};
+  DevParams Pv = P;  // by value in the launch
+  void* args[] = {&Pv, &h->d_state};
   if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
   CK(cudaLaunchCooperativeKernel(k.persist, dim3(P.ntiles), dim3(kThreads), args, smem,
                                  h->stream));
@@ -1131,12 +1147,14 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   } drain{pipe ? h->copy_stream : nullptr};
   unsigned char* ws = h->ws;
 
-  // x0 -> padded device buffer
-  CK(cudaMemsetAsync(ws + L.x0a, 0, es * Dp, h->stream));
-  CK(cudaMemsetAsync(ws + L.x0b, 0, es * Dp, h->stream));
-  CK(cudaMemcpyAsync(ws + L.x0a, x0, es * D,
-                     mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                     h->stream));
+  // x0 -> padded device buffer (x0a and x0b are adjacent: one memset clears both).
+  // The persistent kernel pads x0 itself and reads a device x0 where it lies.
+  if (!persist) CK(cudaMemsetAsync(ws + L.x0a, 0, L.x0b - L.x0a + es * Dp, h->stream));
+  if (!persist || mem == PMCMC_MEM_HOST)
+    CK(cudaMemcpyAsync(ws + L.x0a, x0, es * D,
+                       mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                               : cudaMemcpyHostToDevice,
+                       h->stream));
 
   DevParams P{};
   P.D = D;
@@ -1169,6 +1187,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   P.agg_b = ws + L.agg_b;
   P.incl = ws + L.incl;
   P.colmax = reinterpret_cast<float*>(ws + L.colmax);
+  P.part = reinterpret_cast<double*>(ws + L.part);
   P.xi = reinterpret_cast<float*>(ws + L.xi);
   P.logu = reinterpret_cast<double*>(ws + L.logu);
   if (logistic) {
@@ -1216,6 +1235,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     P.x0 = ws + ((b & 1) ? L.x0b : L.x0a);
     P.x_next = ws + ((b & 1) ? L.x0a : L.x0b);
     P.ncols_out = nkeep;
+    if (persist) {
+      P.x0_src = (b == 0 && mem == PMCMC_MEM_DEVICE) ? x0 : P.x0;
+      P.st_host = pipe ? h->h_states + b : h->h_state;  // written by the kernel
+    }
     if (mem == PMCMC_MEM_DEVICE) {
       P.S_out = static_cast<unsigned char*>(S_out) + es * nsteps * D;
       P.logp_out = logp_out ? static_cast<unsigned char*>(logp_out) + es * nsteps : nullptr;
@@ -1254,12 +1277,14 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     }
     nsteps += nkeep;
     if (pipe) {  // block states are read after the last block
-      CK(cudaMemcpyAsync(h->h_states + b, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
-                         h->stream));
+      if (!persist)
+        CK(cudaMemcpyAsync(h->h_states + b, h->d_state, sizeof(DevState),
+                           cudaMemcpyDeviceToHost, h->stream));
       continue;
     }
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
-                       h->stream));
+    if (!persist)
+      CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                         h->stream));
     CK(cudaStreamSynchronize(h->stream));
     states[static_cast<size_t>(b)] = *h->h_state;
     if (h->h_state->status) break;

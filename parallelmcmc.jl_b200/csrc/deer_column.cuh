@@ -174,7 +174,8 @@ __device__ __forceinline__ void load_params(const DevParams* Pg, DevParams& sp) 
 }
 
 // ---------------------------------------------------------------------------
-// One column, one warp.  Lane owns quads j = lane + 32 q (d = 4j .. 4j+3).
+// One column, one warp (or LPC lanes of it: 32 / LPC columns per warp for the
+// diagonal target).  Lane owns quads j = lane + LPC q (d = 4j .. 4j+3).
 // ---------------------------------------------------------------------------
 template <typename Real, int QPL>
 struct Col {
@@ -203,18 +204,19 @@ __device__ __forceinline__ void load_xi(const DevParams& P, int64_t t, float (&n
   }
 }
 
-template <typename Real, int TK, int QPL>
+template <typename Real, int TK, int QPL, int LPC = 32>
 __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Real>& sm,
                                                const TapeKey& key, const Real* xcol, int t,
                                                Col<Real, QPL>& c,
                                                const float (*xi_pre)[4] = nullptr) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  static_assert(TK == kDiagGauss || LPC == 32, "dense targets use whole warps per column");
+  const int lane = threadIdx.x & (LPC - 1), warp = threadIdx.x >> 5;
   const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
   const Real eps = static_cast<Real>(P.eps), c2 = static_cast<Real>(P.sqrt2eps);
   double la = 0.0;
 #pragma unroll
   for (int q = 0; q < QPL; ++q) {
-    const int j = lane + 32 * q;
+    const int j = lane + LPC * q;
     if (4 * j < D) {
       load4(xcol + 4 * j, c.x[q]);
       float n[4];
@@ -236,7 +238,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     const Real* muR = mean_of<Real>(P);
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lane + LPC * q;
       if (4 * j >= D) {
         // lanes past the last quad take part in the warp reductions with zeros
 #pragma unroll
@@ -272,7 +274,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     double* vd = sm.Vd + warp * Dp;
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lane + LPC * q;
       if (4 * j < D)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
@@ -282,7 +284,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     double gxd[QPL][4];
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lane + LPC * q;
       if (4 * j < D) {
         double o[4];
         matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
@@ -302,7 +304,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lane + LPC * q;
       if (4 * j < D)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
@@ -311,7 +313,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lane + LPC * q;
       if (4 * j < D) {
         double o[4];
         matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
@@ -334,7 +336,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     }
     __syncwarp();
   }
-  c.la = warp_sum(la);
+  c.la = seg_sum<LPC>(la);
 }
 
 // Dense HVP quad: out = -P v (v written to the warp's Real vector first).
@@ -370,12 +372,13 @@ __device__ __forceinline__ void dense_neg_pv(const DevParams& P, const Smem<Real
 }
 
 // Jacobian diagonal estimate A (Real) for one evaluated column.
-template <typename Real, int TK, int JAC, int QPL>
+template <typename Real, int TK, int JAC, int QPL, int LPC = 32>
 __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<Real>& sm,
                                                 const TapeKey& key, int t, int iter, bool acc,
                                                 Real gp, const Col<Real, QPL>& c,
                                                 Real (&A)[QPL][4]) {
-  const int lane = threadIdx.x & 31;
+  static_assert(TK == kDiagGauss || LPC == 32, "dense targets use whole warps per column");
+  const int lane = threadIdx.x & (LPC - 1);
   const int D = static_cast<int>(P.D);
   const Real eps = static_cast<Real>(P.eps), inv2eps = static_cast<Real>(P.inv2eps);
   const Real* lamR = prec_of<Real>(P);
@@ -388,7 +391,7 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
       Real z[QPL][4], w[QPL][4], hvy[QPL][4];
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
-        const int j = lane + 32 * q;
+        const int j = lane + LPC * q;
         if (4 * j < D) {
           const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t),
                                    k, iter);
@@ -404,7 +407,7 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
       if constexpr (TK == kDiagGauss) {
 #pragma unroll
         for (int q = 0; q < QPL; ++q) {
-          const int j = lane + 32 * q;
+          const int j = lane + LPC * q;
           Real lam[4] = {0, 0, 0, 0};
           if (4 * j < D) load4(lamR + 4 * j, lam);
 #pragma unroll
@@ -431,7 +434,7 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
           const Real dr = z[q][e] - w[q][e] - eps * hvy[q][e];
           dla += c.gy[q][e] * w[q][e] - c.gx[q][e] * z[q][e] - inv2eps * r * dr;
         }
-      dla = warp_sum(dla);
+      dla = seg_sum<LPC>(dla);
       const Real dg = gp * dla;
 #pragma unroll
       for (int q = 0; q < QPL; ++q)
@@ -454,7 +457,7 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
     if constexpr (TK == kDiagGauss) {
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
-        const int j = lane + 32 * q;
+        const int j = lane + LPC * q;
         Real lam[4] = {0, 0, 0, 0};
         if (4 * j < D) load4(lamR + 4 * j, lam);
 #pragma unroll
@@ -478,7 +481,7 @@ __device__ __forceinline__ void column_jacobian(const DevParams& P, const Smem<R
       const int Dp = static_cast<int>(P.Dp);
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
-        const int j = lane + 32 * q;
+        const int j = lane + LPC * q;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int i = 4 * j + e;

@@ -21,6 +21,8 @@ enum DevStatus : int32_t { kStOk = 0, kStNonfinite = 4, kStTimeout = 5 };
 
 // Everything a solve needs, resident in device memory so that one captured
 // CUDA graph serves every call (kernels copy it to shared memory on entry).
+struct DevState;
+
 struct DevParams {
   int64_t D, Dp, T, W;  // Dp = D rounded up to 4; W = window width (T if none)
   int64_t ncols_out;    // columns copied to S_out by the finalize pass
@@ -61,6 +63,10 @@ struct DevParams {
   // padded rows zero) and log(u_t) in FP64
   float* xi;
   double* logu;
+  // persistent solve (deer_persist.cu)
+  double* part;         // [2 * ntiles * 4] per-CTA partial reductions
+  const void* x0_src;   // start state as given (D entries, unpadded), or nullptr: use x0
+  DevState* st_host;    // pinned host copy of the final state (nullptr: none)
 };
 
 struct DevState {
@@ -91,6 +97,21 @@ __device__ __forceinline__ T warp_sum(T v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Sum / max over aligned groups of W lanes (W a power of two <= 32); every
+// lane of the warp takes part.
+template <int W, typename T>
+__device__ __forceinline__ T seg_sum(T v) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int W, typename T>
+__device__ __forceinline__ T seg_max(T v) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_max(T v) {
 #pragma unroll

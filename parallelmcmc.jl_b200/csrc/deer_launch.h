@@ -26,10 +26,10 @@ struct SweepKernels {
 // plan at TT columns plus the CTA's tape (TT + 1 columns of xi and log u).
 struct PersistPlan {
   SmemPlan sweep;
-  size_t xi, lu, total;
+  size_t xi, lu, x0, total;
 };
 PersistPlan persist_smem(bool f64, int64_t Dp, int TT, bool dense);
-const void* persist_kernel(bool f64, int tk, int jac, int qpl);
+const void* persist_kernel(bool f64, int tk, int jac, int64_t D);
 
 // Raises a kernel's dynamic shared-memory limit to at least `bytes`, never
 // lowering it: the attribute is global per function, and handles on other

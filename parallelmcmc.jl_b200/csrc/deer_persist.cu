@@ -21,6 +21,8 @@
 //    (_trajectory_logps, interface.jl:517-524), as the finalize kernel does.
 // The kernel is used when every CTA is co-resident (cooperative launch), the
 // block has no sliding window and the target is a diagonal or dense Gaussian.
+// Its parameters come by value in the launch, so a solve is one launch and
+// the state readback.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -46,6 +48,8 @@ __host__ __device__ inline PersistPlan plan_persist_smem(int64_t Dp, int TT, boo
   off = al(off + sizeof(float) * (TT + 1) * Dp);
   p.lu = off;
   off = al(off + sizeof(double) * (TT + 1));
+  p.x0 = off;
+  off = al(off + sizeof(Real) * Dp);
   p.total = off;
   return p;
 }
@@ -56,12 +60,12 @@ PersistPlan persist_smem(bool f64, int64_t Dp, int TT, bool dense) {
 
 namespace {
 
-template <int QPL>
+template <int QPL, int LPC>
 __device__ __forceinline__ void xi_from_smem(const float* col, int D, float (&n)[QPL][4]) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (LPC - 1);
 #pragma unroll
   for (int q = 0; q < QPL; ++q) {
-    const int j = lane + 32 * q;
+    const int j = lane + LPC * q;
     if (4 * j < D) {
       load4(col + 4 * j, n[q]);
     } else {
@@ -71,25 +75,59 @@ __device__ __forceinline__ void xi_from_smem(const float* col, int D, float (&n)
   }
 }
 
-__device__ __forceinline__ unsigned long long ld_l2(const unsigned long long* p) {
-  return __ldcg(p);
+// Block-wide maxima of the three partials part[4 c + 0..2] over c < n (every
+// CTA's slot): the same result in every CTA that calls it.
+__device__ __forceinline__ void reduce_partials(const double* part, int n, double* s_red,
+                                                double& a, double& b, double& c) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double x = -INFINITY, y = -INFINITY, z = -INFINITY;
+  for (int i = tid; i < n; i += kThreads) {
+    x = max(x, __ldcg(part + 4 * i));
+    y = max(y, __ldcg(part + 4 * i + 1));
+    z = max(z, __ldcg(part + 4 * i + 2));
+  }
+  x = warp_max(x);
+  y = warp_max(y);
+  z = warp_max(z);
+  __syncthreads();  // s_red may still be read from the previous use
+  if (lane == 0) {
+    s_red[warp] = x;
+    s_red[kWarps + warp] = y;
+    s_red[2 * kWarps + warp] = z;
+  }
+  __syncthreads();
+  a = b = c = -INFINITY;
+  for (int w = 0; w < kWarps; ++w) {
+    a = max(a, s_red[w]);
+    b = max(b, s_red[kWarps + w]);
+    c = max(c, s_red[2 * kWarps + w]);
+  }
 }
 
 }  // namespace
 
-template <typename Real, int TK, int JAC, int QPL>
-__global__ void __launch_bounds__(kThreads)
-    deer_persist_kernel(const DevParams* __restrict__ Pg, DevState* __restrict__ st) {
+// Two CTAs per SM (at most 128 registers a thread) where that costs no spills:
+// FP32 state with up to two quads a lane, FP64 with one.
+template <typename Real, int QPL>
+constexpr int kPersistMinBlocks = sizeof(Real) * QPL <= 8 ? 2 : 1;
+
+// Columns are evaluated by LPC lanes each (32 / LPC columns per warp); QPL
+// quads per lane cover Dp / 4 <= LPC * QPL.
+template <typename Real, int TK, int JAC, int QPL, int LPC>
+__global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
+    deer_persist_kernel(const DevParams Pv, DevState* __restrict__ st) {
   __shared__ DevParams P;
   __shared__ Real s_sa[kThreads], s_sb[kThreads];
   __shared__ double s_red[3][kWarps];
   __shared__ unsigned long long s_acc[kWarps];
-  __shared__ int s_bad;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  load_params(Pg, P);
+  if (threadIdx.x == 0) P = Pv;  // parameters by value: no upload before the launch
+  __syncthreads();
   cg::grid_group grid = cg::this_grid();
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int CPW = 32 / LPC;                  // columns per warp
+  const int lq = lane & (LPC - 1), half = lane / LPC;  // quad lane, column slot
   const int cta = static_cast<int>(blockIdx.x), nctas = static_cast<int>(gridDim.x);
   const int TT = P.tile_cols;
   const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
@@ -103,65 +141,52 @@ __global__ void __launch_bounds__(kThreads)
   const PersistPlan pp = plan_persist_smem<Real>(Dp, TT, kDense);
   float* xis = reinterpret_cast<float*>(smem_raw + pp.xi);
   double* lus = reinterpret_cast<double*>(smem_raw + pp.lu);
-  const Real* x0 = static_cast<const Real*>(P.x0);
   Real* agg_a = static_cast<Real*>(P.agg_a);
   Real* agg_b = static_cast<Real*>(P.agg_b);
   Real* incl = static_cast<Real*>(P.incl);
   Real* carry0 = incl + static_cast<size_t>(nctas) * Dp;  // S_0 = f(x0)
   Real* Sb = static_cast<Real*>(P.S[0]);                   // last column of every CTA
 
-  if (cta == 0 && tid == 0) {
-    st->iter = 0;
-    st->cur = 0;
-    st->converged = 0;
-    st->status = 0;
-    st->t_lo = 0;
-    st->t_lo_prev = 0;
-    st->dmax_bits = 0;
-    st->smax_bits = 0;
-    st->metric = __longlong_as_double(0x7ff0000000000000ll);
-    st->n_accept = 0;
-    st->min_margin_bits = 0x7ff0000000000000ull;  // +inf
-    st->max_defect_bits = 0;
+  double* part = P.part;  // [c][4]: this sweep's max|dS|, max|S|, non-finite flag
+  double* part_fin = P.part + 4 * static_cast<size_t>(nctas);  // accepts, margin, defect
+  Real* x0s = reinterpret_cast<Real*>(smem_raw + pp.x0);
+  {  // start state, zero-padded to Dp
+    const Real* src = static_cast<const Real*>(P.x0_src ? P.x0_src : P.x0);
+    for (int d = tid; d < Dp; d += kThreads) x0s[d] = d < D ? src[d] : Real(0);
   }
-  if (tid == 0) s_bad = 0;
 
-  // ---- tape of columns t0 .. t0 + ncols (interface.jl:334-358) and S = x0 ----
+  // ---- tape (interface.jl:334-358) of column t0 here; columns t0 + 1 ..
+  // t0 + ncols are drawn by the first sweep's evaluation, which uses them first ----
   const TapeKey key(P.seed, P.block);
-  {
-    const int nq = Dp / 4;
-    const int ntape = has_next ? ncols + 1 : ncols;
-    for (int i = tid; i < ntape * nq; i += kThreads) {
-      const int c = i / nq, q = i - c * nq;
-      const uint32_t tg = static_cast<uint32_t>(t0 + c + P.t_off);
-      float n[4];
-      tape_xi4(key, static_cast<uint32_t>(q), tg, n);
+  for (int q = tid; q < Dp / 4; q += kThreads) {
+    const uint32_t tg = static_cast<uint32_t>(t0 + P.t_off);
+    float n[4];
+    tape_xi4(key, static_cast<uint32_t>(q), tg, n);
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (4 * q + e >= D) n[e] = 0.f;
-      store4(xis + c * Dp + 4 * q, n);
-      if (q == 0) lus[c] = log(static_cast<double>(tape_u(key, tg)));
-    }
-    for (int i = tid; i < ncols * nq; i += kThreads) {
-      const int c = i / nq, k = 4 * (i - c * nq);
-      Real v[4];
-      load4(x0 + k, v);
-      store4(sm.Xs + c * Dp + k, v);
-    }
+    for (int e = 0; e < 4; ++e)
+      if (4 * q + e >= D) n[e] = 0.f;
+    store4(xis + 4 * q, n);
+    if (q == 0) lus[0] = log(static_cast<double>(tape_u(key, tg)));
   }
   __syncthreads();
+  for (int i = tid; i < ncols * (Dp / 4); i += kThreads) {
+    const int nq = Dp / 4, c = i / nq, k = 4 * (i - c * nq);
+    Real v[4];
+    load4(x0s + k, v);
+    store4(sm.Xs + c * Dp + k, v);
+  }
 
   // ---- S_0 = f(x0): the same in every sweep ----
-  if (cta == 0 && warp == 0) {
+  if (cta == 0 && warp == 0) {  // every column slot of warp 0 forms it; slot 0 stores
     float xic[QPL][4];
-    xi_from_smem<QPL>(xis, D, xic);
+    xi_from_smem<QPL, LPC>(xis, D, xic);
     Col<Real, QPL> col;
-    column_forward<Real, TK, QPL>(P, sm, key, x0, 0, col, xic);
+    column_forward<Real, TK, QPL, LPC>(P, sm, key, x0s, 0, col, xic);
     const bool acc = lus[0] < col.la;
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
-      if (4 * j < D) {
+      const int j = lq + LPC * q;
+      if (half == 0 && 4 * j < D) {
         Real f[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) f[e] = 4 * j + e < D ? (acc ? col.y[q][e] : col.x[q][e]) : Real(0);
@@ -172,26 +197,53 @@ __global__ void __launch_bounds__(kThreads)
 
   const Real dmp = static_cast<Real>(P.damping), omd = static_cast<Real>(1.0 - P.damping);
   const bool undamped = P.damping == 1.0;
-  int iter = 0, converged = 0;
+  int iter = 0, converged = 0, status = 0;
   double metric = 0.0;
   for (;;) {
     // ---- evaluate the scan group: column t0 + c + 1 from S_{t0 + c} ----
-    for (int c = warp; c < ng; c += kWarps) {
+    // (warp-uniform loop over groups of CPW columns; a slot past the end
+    // repeats the group's first column and stores nothing)
+    for (int cb = warp * CPW; cb < ng; cb += kWarps * CPW) {
+      const bool valid = cb + half < ng;
+      const int c = valid ? cb + half : cb;
       const int t = static_cast<int>(t0 + c + 1);
       float xic[QPL][4];
-      xi_from_smem<QPL>(xis + (c + 1) * Dp, D, xic);
+      double logu;
+      if (iter == 0) {
+        // first use of column t's tape: drawn here, kept in shared memory
+        const uint32_t tg = static_cast<uint32_t>(t + P.t_off);
+#pragma unroll
+        for (int q = 0; q < QPL; ++q) {
+          const int j = lq + LPC * q;
+          if (4 * j < D) {
+            tape_xi4(key, static_cast<uint32_t>(j), tg, xic[q]);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (4 * j + e >= D) xic[q][e] = 0.f;
+            if (valid) store4(xis + (c + 1) * Dp + 4 * j, xic[q]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) xic[q][e] = 0.f;
+          }
+        }
+        const double lu = lq == 0 ? log(static_cast<double>(tape_u(key, tg))) : 0.0;
+        logu = __shfl_sync(0xffffffffu, lu, half * LPC);
+        if (valid && lq == 0) lus[c + 1] = logu;
+      } else {
+        xi_from_smem<QPL, LPC>(xis + (c + 1) * Dp, D, xic);
+        logu = lus[c + 1];
+      }
       Col<Real, QPL> col;
-      column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
-      const double logu = lus[c + 1];
+      column_forward<Real, TK, QPL, LPC>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
       const bool acc = logu < col.la;
       const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
       const Real gp = static_cast<Real>(gd * (1.0 - gd));
       Real A[QPL][4];
-      column_jacobian<Real, TK, JAC, QPL>(P, sm, key, t + P.t_off, iter, acc, gp, col, A);
+      column_jacobian<Real, TK, JAC, QPL, LPC>(P, sm, key, t + P.t_off, iter, acc, gp, col, A);
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
-        const int j = lane + 32 * q;
-        if (4 * j < D) {
+        const int j = lq + LPC * q;
+        if (valid && 4 * j < D) {
           Real a4[4], b4[4];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -212,11 +264,6 @@ __global__ void __launch_bounds__(kThreads)
       agg_b[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.Bs[(ng - 1) * Dp + d] : Real(0);
     }
     grid.sync();
-    // every CTA has read the previous sweep's maxima: clear them for this one
-    if (cta == 0 && tid == 0) {
-      st->dmax_bits = 0;
-      st->smax_bits = 0;
-    }
 
     // ---- state entering every CTA: scan of the group aggregates per coordinate ----
     for (int d = cta; d < D; d += nctas)
@@ -263,67 +310,75 @@ __global__ void __launch_bounds__(kThreads)
         }
       }
     }
-    if (bad) s_bad = 1;
+    // this CTA's partials: plain stores to its own slot (no contended atomics)
     my_dmax = warp_max(my_dmax);
     my_smax = warp_max(my_smax);
+    bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
       s_red[0][warp] = my_dmax;
       s_red[1][warp] = my_smax;
+      s_red[2][warp] = bad ? 1.0 : 0.0;
     }
     __syncthreads();
     if (tid == 0) {
-      double a = 0, b = 0;
-      for (int w = 0; w < kWarps; ++w) a = max(a, s_red[0][w]), b = max(b, s_red[1][w]);
-      if (a > 0) atomicMax(&st->dmax_bits, dbits(a));
-      if (b > 0) atomicMax(&st->smax_bits, dbits(b));
-      if (s_bad) atomicCAS(&st->status, 0, static_cast<int>(kStNonfinite));
+      double a = 0, b = 0, c = 0;
+      for (int w = 0; w < kWarps; ++w)
+        a = max(a, s_red[0][w]), b = max(b, s_red[1][w]), c = max(c, s_red[2][w]);
+      part[4 * cta] = a;
+      part[4 * cta + 1] = b;
+      part[4 * cta + 2] = c;
     }
     grid.sync();
 
     // ---- convergence test (DEER.jl:567-578), the same in every CTA ----
-    const double dmax = bitsd(ld_l2(&st->dmax_bits));
-    const double smax = bitsd(ld_l2(&st->smax_bits));
-    const int status = __ldcg(&st->status);
+    double dmax, smax, nonfinite;
+    reduce_partials(part, nctas, &s_red[0][0], dmax, smax, nonfinite);
     metric = dmax / (P.tol_abs + P.tol_rel * smax);
     ++iter;
     converged = metric <= 1.0;
+    status = nonfinite != 0.0 ? static_cast<int>(kStNonfinite) : 0;
     if (converged || iter >= P.maxiter || status != 0) break;
   }
 
   // ---- verification pass and outputs on the CTA's columns ----
   // S_{t0 - 1}, the previous CTA's last column, into shared memory
   for (int d = tid; d < Dp; d += kThreads)
-    sm.carry[d] = cta == 0 ? x0[d] : __ldcg(Sb + (t0 - 1) * Dp + d);
+    sm.carry[d] = cta == 0 ? x0s[d] : __ldcg(Sb + (t0 - 1) * Dp + d);
   __syncthreads();
   unsigned long long nacc = 0;
   double min_margin = __longlong_as_double(0x7ff0000000000000ll), max_def = 0.0;
-  for (int c = warp; c < ncols; c += kWarps) {
+  for (int cb = warp * CPW; cb < ncols; cb += kWarps * CPW) {
+    const bool valid = cb + half < ncols;
+    const int c = valid ? cb + half : cb;
     const int64_t t = t0 + c;
     const Real* xcol = c == 0 ? sm.carry : sm.Xs + (c - 1) * Dp;
     const Real* scol = sm.Xs + c * Dp;
     float xic[QPL][4];
-    xi_from_smem<QPL>(xis + c * Dp, D, xic);
+    xi_from_smem<QPL, LPC>(xis + c * Dp, D, xic);
     Col<Real, QPL> col;
-    column_forward<Real, TK, QPL>(P, sm, key, xcol, static_cast<int>(t), col, xic);
+    column_forward<Real, TK, QPL, LPC>(P, sm, key, xcol, static_cast<int>(t), col, xic);
     const double logu = lus[c];
     const bool acc = logu < col.la;
-    double def = 0.0, lp = 0.0;
+    const bool out = valid && t < P.ncols_out;
+    // the recursion defect max|S_t - f_t| for both outcomes, selected after the
+    // reductions (which then run alongside the log-density's)
+    double dx = 0.0, dy = 0.0, lp = 0.0;
     double* vd = kDense ? sm.Vd + warp * Dp : nullptr;
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
-      const int j = lane + 32 * q;
+      const int j = lq + LPC * q;
       if (4 * j < D) {
         Real s4[4];
         load4(scol + 4 * j, s4);
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           if (4 * j + e >= D) continue;
-          const Real f = acc ? col.y[q][e] : col.x[q][e];
-          def = max(def, static_cast<double>(fabs(s4[e] - f)));
+          dx = max(dx, static_cast<double>(fabs(s4[e] - col.x[q][e])));
+          dy = max(dy, static_cast<double>(fabs(s4[e] - col.y[q][e])));
           const double sd = static_cast<double>(s4[e]) - P.mean_d[4 * j + e];
           if constexpr (TK == kDiagGauss) lp += -0.5 * P.prec_d[4 * j + e] * sd * sd;
           else vd[4 * j + e] = sd;
-          if (t < P.ncols_out) {
+          if (out) {
             static_cast<Real*>(P.S_out)[t * D + 4 * j + e] = s4[e];
             if (t == P.ncols_out - 1) static_cast<Real*>(P.x_next)[4 * j + e] = s4[e];
           }
@@ -334,7 +389,7 @@ __global__ void __launch_bounds__(kThreads)
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < QPL; ++q) {
-        const int j = lane + 32 * q;
+        const int j = lq + LPC * q;
         if (4 * j < D) {
           double o[4];
           matvec4<double, double, double>(sm.Pd, vd, D, Dp, j, o);
@@ -345,18 +400,29 @@ __global__ void __launch_bounds__(kThreads)
       }
       __syncwarp();
     }
-    lp = warp_sum(lp);
-    def = warp_max(def);
-    if (lane == 0) {
-      if (t < P.ncols_out) {
+#pragma unroll
+    for (int o = LPC / 2; o > 0; o >>= 1) {
+      lp += __shfl_xor_sync(0xffffffffu, lp, o);
+      dx = max(dx, __shfl_xor_sync(0xffffffffu, dx, o));
+      dy = max(dy, __shfl_xor_sync(0xffffffffu, dy, o));
+    }
+    if (valid && lq == 0) {
+      if (out) {
         if (P.logp_out) static_cast<Real*>(P.logp_out)[t] = static_cast<Real>(lp);
         if (P.accept_out) P.accept_out[t] = acc ? 1 : 0;
       }
       nacc += acc ? 1 : 0;
       min_margin = min(min_margin, fabs(col.la - logu));
-      max_def = max(max_def, def);
+      max_def = max(max_def, acc ? dy : dx);
     }
   }
+  // per warp: the column slots' totals
+  nacc = warp_sum(nacc);
+  max_def = warp_max(max_def);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    min_margin = min(min_margin, __shfl_xor_sync(0xffffffffu, min_margin, o));
+  __syncthreads();  // s_red was last read in the convergence test
   if (lane == 0) {
     s_acc[warp] = nacc;
     s_red[0][warp] = min_margin;
@@ -371,13 +437,39 @@ __global__ void __launch_bounds__(kThreads)
       mm = min(mm, s_red[0][w]);
       md = max(md, s_red[2][w]);
     }
-    if (a) atomicAdd(&st->n_accept, a);
-    atomicMin(&st->min_margin_bits, dbits(mm));
-    if (md > 0) atomicMax(&st->max_defect_bits, dbits(md));
-    if (cta == 0) {
-      st->iter = iter;
-      st->converged = converged;
-      st->metric = metric;
+    // accepted count (exact in a double), -margin (so that max is min), defect
+    part_fin[4 * cta] = static_cast<double>(a);
+    part_fin[4 * cta + 1] = -mm;
+    part_fin[4 * cta + 2] = md;
+  }
+  grid.sync();
+  if (cta != 0) return;
+
+  // ---- CTA 0: totals of the verification pass and the final state ----
+  double nacc_tot = 0.0;
+  for (int i = tid; i < nctas; i += kThreads) nacc_tot += __ldcg(part_fin + 4 * i);
+  nacc_tot = warp_sum(nacc_tot);
+  __syncthreads();
+  if (lane == 0) s_red[1][warp] = nacc_tot;
+  __syncthreads();
+  double tot = 0.0;
+  for (int w = 0; w < kWarps; ++w) tot += s_red[1][w];
+  double neg_mm, maxdef, unused;
+  reduce_partials(part_fin, nctas, &s_red[0][0], unused, neg_mm, maxdef);
+  if (tid == 0) {
+    DevState f{};
+    f.epoch = st->epoch;  // look-back epochs of the per-sweep path continue
+    f.iter = iter;
+    f.converged = converged;
+    f.status = status;
+    f.metric = metric;
+    f.n_accept = static_cast<unsigned long long>(tot);
+    f.min_margin_bits = dbits(-neg_mm);
+    f.max_defect_bits = dbits(maxdef);
+    *st = f;
+    if (P.st_host) {
+      *P.st_host = f;
+      __threadfence_system();
     }
   }
 }
@@ -385,28 +477,32 @@ __global__ void __launch_bounds__(kThreads)
 namespace {
 
 template <typename Real, int TK, int JAC>
-const void* pick_persist(int qpl) {
-  switch (qpl) {
-    case 1: return reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 1>);
-    case 2: return reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 2>);
-    default: return reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 4>);
+const void* pick_persist(int64_t D) {
+  const void* k = nullptr;
+  if constexpr (TK == kDiagGauss) {  // two columns per warp while D <= 128
+    if (D <= 64) return reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 1, 16>);
+    if (D <= 128) return reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 2, 16>);
   }
+  if (D <= 128) k = reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 1, 32>);
+  else if (D <= 256) k = reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 2, 32>);
+  else k = reinterpret_cast<const void*>(&deer_persist_kernel<Real, TK, JAC, 4, 32>);
+  return k;
 }
 
 template <typename Real>
-const void* pick_persist_t(int tk, int jac, int qpl) {
+const void* pick_persist_t(int tk, int jac, int64_t D) {
   if (tk == kDiagGauss)
-    return jac == kJacStoch ? pick_persist<Real, kDiagGauss, kJacStoch>(qpl)
-                            : pick_persist<Real, kDiagGauss, kJacDiag>(qpl);
-  return jac == kJacStoch ? pick_persist<Real, kDenseGauss, kJacStoch>(qpl)
-                          : pick_persist<Real, kDenseGauss, kJacDiag>(qpl);
+    return jac == kJacStoch ? pick_persist<Real, kDiagGauss, kJacStoch>(D)
+                            : pick_persist<Real, kDiagGauss, kJacDiag>(D);
+  return jac == kJacStoch ? pick_persist<Real, kDenseGauss, kJacStoch>(D)
+                          : pick_persist<Real, kDenseGauss, kJacDiag>(D);
 }
 
 }  // namespace
 
-const void* persist_kernel(bool f64, int tk, int jac, int qpl) {
+const void* persist_kernel(bool f64, int tk, int jac, int64_t D) {
   if (tk != kDiagGauss && tk != kDenseGauss) return nullptr;
-  return f64 ? pick_persist_t<double>(tk, jac, qpl) : pick_persist_t<float>(tk, jac, qpl);
+  return f64 ? pick_persist_t<double>(tk, jac, D) : pick_persist_t<float>(tk, jac, D);
 }
 
 }  // namespace pmcmc

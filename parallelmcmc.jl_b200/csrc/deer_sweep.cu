@@ -746,7 +746,7 @@ SweepKernels logistic_sweep_kernels(bool f64, int64_t D) {
 SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D) {
   const int qpl = D <= 128 ? 1 : (D <= 256 ? 2 : 4);
   SweepKernels k = f64 ? pick1<double>(tk, jac, qpl) : pick1<float>(tk, jac, qpl);
-  k.persist = persist_kernel(f64, tk, jac, qpl);
+  k.persist = persist_kernel(f64, tk, jac, D);
   k.qpl = qpl;
   return k;
 }

@@ -29,6 +29,14 @@ def _is_torch_cuda(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+def _torch_ready(x):
+    """Wait for torch's current stream on x's device: the library runs on its
+    handle's stream, which is not ordered after torch's work on x."""
+    import torch
+    torch.cuda.current_stream(x.device).synchronize()
+    return x
+
+
 def _dtype_code(dt) -> int:
     return L.F32 if np.dtype(dt) == np.float32 else L.F64
 
@@ -233,6 +241,7 @@ def _input_vector(x, D, dtype, device_like):
         x = x.detach().to(dtype=tdt).contiguous().reshape(-1)
         if x.numel() != D:
             raise DimensionMismatch(f"initial state must have length {D}")
+        _torch_ready(x)
         return x, x.data_ptr(), L.MEM_DEVICE
     a = np.ascontiguousarray(np.asarray(x, dtype=dtype).ravel())
     if a.size != D:
@@ -393,7 +402,7 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
     tgt = model.device_target(h)
     keep, x0p, mem = _input_vector(s0, model.dim, sampler.dtype, None)
     if mem == L.MEM_DEVICE:
-        Sc = S.T.contiguous()
+        Sc = _torch_ready(S.T.contiguous())
         sp = Sc.data_ptr()
     else:
         Sc = np.ascontiguousarray(np.asarray(S).T, dtype=np.float32)
@@ -485,6 +494,7 @@ def solve_affine_scan_diag(A, B, s0, *, handle: Optional[L.Handle] = None, devic
         Bc = B.to(dt).T.contiguous()
         sc = s0.to(dt).contiguous()
         S = torch.empty_like(Ac)
+        _torch_ready(Ac)
         rc = lib.pmcmc_affine_scan_diag(h.ptr, L.F32 if dt == torch.float32 else L.F64, D, T,
                                         Ac.data_ptr(), Bc.data_ptr(), sc.data_ptr(),
                                         S.data_ptr(), L.MEM_DEVICE)

@@ -282,9 +282,9 @@ def _persist_cases():
         ("diag_f32", pmcmc.DensityModel.diag_gaussian(lam),
          dict(T=2048, jacobian="diag", dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6), x100,
          0, 1e-5),
+        # the sampler's default stopping rule (1e-6 + 1e-5 |S|), well above FP32 resolution
         ("stoch_f32_odd_T", pmcmc.DensityModel.diag_gaussian(lam),
-         dict(T=2047, jacobian="stoch_diag", dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6,
-              maxiter=1000), x100, 4, 1e-5),
+         dict(T=2047, jacobian="stoch_diag", dtype=np.float32, maxiter=1000), x100, 3, 1e-4),
         # default stopping rule with damping 0.5: the last column stops ~tol from f(x)
         ("diag_f64_D3_T1", pmcmc.DensityModel.diag_gaussian(np.ones(3)),
          dict(T=1, jacobian="diag"), np.ones(3), 0, 1e-4),
@@ -317,6 +317,7 @@ def test_persistent_solve_matches_graph_path(monkeypatch, case):
     assert np.array_equal(ap, ag), name
     assert ip["n_accept"] == ig["n_accept"]
     tol = 2e-5 if sampler.dtype == np.float32 else 1e-10
+    tol = max(tol, bar)  # both stop within the stopping rule of the same fixed point
     assert trace_err(Sp, Sg) <= tol, name
     np.testing.assert_allclose(lpp, lpg, rtol=tol, atol=tol * np.abs(lpg).max())
     tg = _oracle_target(model)
