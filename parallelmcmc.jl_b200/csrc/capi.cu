@@ -293,17 +293,20 @@ TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t D
   return tp;
 }
 
-// Columns per CTA of the persistent solve: the smallest power of two whose
-// tiles are all co-resident (one cooperative launch); 0 when none is.
+// Columns per CTA of the persistent solve: the most CTAs a SM whose tiles all
+// fit co-resident (one cooperative launch), TT = ceil(T / (CTAs a SM x SMs));
+// 0 when none fits.
 int choose_persist_tile(pmcmc_handle* h, const void* fn, bool f64, int64_t Dp, int64_t T,
                         bool dense) {
   if (!fn || h->no_coop || h->tile_override > 0) return 0;
-  for (int TT = 8; TT <= 256; TT <<= 1) {
-    const size_t smem = persist_smem(f64, Dp, TT, dense).total;
-    if (smem > 200 * 1024) break;
+  for (int per_sm = 8; per_sm >= 1; --per_sm) {
+    const int64_t TT = (T + int64_t(per_sm) * h->num_sms - 1) / (int64_t(per_sm) * h->num_sms);
+    if (TT > 256) break;
+    const size_t smem = persist_smem(f64, Dp, static_cast<int>(TT), dense).total;
+    if (smem > 200 * 1024) continue;
     const int nb = max_active_blocks(fn, smem);
     if (nb < 0) return 0;
-    if (nb > 0 && (T + TT - 1) / TT <= static_cast<int64_t>(nb) * h->num_sms) return TT;
+    if (nb >= per_sm) return static_cast<int>(TT);
   }
   return 0;
 }
