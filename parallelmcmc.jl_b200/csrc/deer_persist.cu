@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     grid.sync();
 
     // ---- apply: Newton state of every column, damping, maxima ----
-    double my_dmax = 0.0, my_smax = 0.0;
+    Real my_dmax = 0, my_smax = 0;  // maxima are exact in the state's precision
     bool bad = false;
     Real cr[QPL][4];
 #pragma unroll
@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
             const Real s = a4[e] * cr[q][e] + b4[e];
             n4[e] = undamped ? s : omd * o4[e] + dmp * s;
             if (4 * j + e < D) {
-              my_dmax = max(my_dmax, static_cast<double>(fabs(n4[e] - o4[e])));
-              my_smax = max(my_smax, static_cast<double>(fabs(n4[e])));
+              my_dmax = max(my_dmax, fabs(n4[e] - o4[e]));
+              my_smax = max(my_smax, fabs(n4[e]));
               bad |= !isfinite(n4[e]);
             } else {
               n4[e] = Real(0);
@@ -315,8 +315,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     my_smax = warp_max(my_smax);
     bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
-      s_red[0][warp] = my_dmax;
-      s_red[1][warp] = my_smax;
+      s_red[0][warp] = static_cast<double>(my_dmax);
+      s_red[1][warp] = static_cast<double>(my_smax);
       s_red[2][warp] = bad ? 1.0 : 0.0;
     }
     __syncthreads();
@@ -344,6 +344,26 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
   // S_{t0 - 1}, the previous CTA's last column, into shared memory
   for (int d = tid; d < Dp; d += kThreads)
     sm.carry[d] = cta == 0 ? x0s[d] : __ldcg(Sb + (t0 - 1) * Dp + d);
+  // the CTA's rows of S_out (row t = column t, D entries) in one coalesced copy
+  {
+    const int64_t nrows = imin64(ncols, P.ncols_out - t0);
+    if (nrows > 0) {
+      Real* dst = static_cast<Real*>(P.S_out) + t0 * D;
+      const int64_t n = nrows * D;
+      if (D == Dp && reinterpret_cast<uintptr_t>(dst) % (4 * sizeof(Real)) == 0) {
+        for (int64_t i = tid; i < n / 4; i += kThreads) {
+          Real v[4];
+          load4(sm.Xs + 4 * i, v);
+          store4(dst + 4 * i, v);
+        }
+      } else {
+        for (int64_t i = tid; i < n; i += kThreads) {
+          const int64_t r = i / D;
+          dst[i] = sm.Xs[r * Dp + (i - r * D)];
+        }
+      }
+    }
+  }
   __syncthreads();
   unsigned long long nacc = 0;
   double min_margin = __longlong_as_double(0x7ff0000000000000ll), max_def = 0.0;
@@ -362,7 +382,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     const bool out = valid && t < P.ncols_out;
     // the recursion defect max|S_t - f_t| for both outcomes, selected after the
     // reductions (which then run alongside the log-density's)
-    double dx = 0.0, dy = 0.0, lp = 0.0;
+    Real dx = 0, dy = 0;  // exact maxima
+    double lp = 0.0;
     double* vd = kDense ? sm.Vd + warp * Dp : nullptr;
 #pragma unroll
     for (int q = 0; q < QPL; ++q) {
@@ -373,15 +394,12 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           if (4 * j + e >= D) continue;
-          dx = max(dx, static_cast<double>(fabs(s4[e] - col.x[q][e])));
-          dy = max(dy, static_cast<double>(fabs(s4[e] - col.y[q][e])));
+          dx = max(dx, fabs(s4[e] - col.x[q][e]));
+          dy = max(dy, fabs(s4[e] - col.y[q][e]));
           const double sd = static_cast<double>(s4[e]) - P.mean_d[4 * j + e];
           if constexpr (TK == kDiagGauss) lp += -0.5 * P.prec_d[4 * j + e] * sd * sd;
           else vd[4 * j + e] = sd;
-          if (out) {
-            static_cast<Real*>(P.S_out)[t * D + 4 * j + e] = s4[e];
-            if (t == P.ncols_out - 1) static_cast<Real*>(P.x_next)[4 * j + e] = s4[e];
-          }
+          if (out && t == P.ncols_out - 1) static_cast<Real*>(P.x_next)[4 * j + e] = s4[e];
         }
       }
     }
@@ -413,7 +431,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       }
       nacc += acc ? 1 : 0;
       min_margin = min(min_margin, fabs(col.la - logu));
-      max_def = max(max_def, acc ? dy : dx);
+      max_def = max(max_def, static_cast<double>(acc ? dy : dx));
     }
   }
   // per warp: the column slots' totals
