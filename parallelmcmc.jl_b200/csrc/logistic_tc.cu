@@ -16,9 +16,9 @@
 // hi*hi + hi*lo + lo*hi with FP32 accumulation.  Tangent columns (only used
 // for the Jacobian estimate) and s use a single FP16 term.
 //
-// Roles: warps 0-7 run the epilogue (warps w and w+4 share TMEM lane quarter
-// w % 4 and split the columns); lane 0 of warp 8 issues TMA loads and MMAs
-// and warp 8 owns the TMEM allocation.
+// Roles: warps 0-15 run the epilogue (warps w, w+4, w+8, w+12 share TMEM lane
+// quarter w % 4 and take 8 columns each); lane 0 of warp 16 issues TMA loads
+// and MMAs and warp 16 owns the TMEM allocation.
 // Every mbarrier wait is bounded; on timeout the kernel records an error,
 // drains its own MMAs and frees TMEM before returning.
 #include <cuda.h>
@@ -37,9 +37,10 @@ namespace tc {
 
 constexpr int BN = 128;  // data rows per block (GEMM1 M)
 constexpr int BT = 32;   // value columns per CTA (plus BT tangent columns)
-constexpr int kThreadsTC = 288;  // 8 epilogue warps + 1 producer warp
-constexpr int kEpi = 8;
-constexpr int kProd = 8;  // producer / TMEM-owner warp
+constexpr int kThreadsTC = 544;  // 16 epilogue warps + 1 producer warp
+constexpr int kEpi = 16;
+constexpr int kProd = 16;  // producer / TMEM-owner warp
+constexpr int kParts = kEpi / 4;  // epilogue warps per TMEM lane quarter
 constexpr uint32_t kTmemCols = 256;
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
 constexpr uint32_t kBoxX = BN * 128;       // one 64-wide d box of X: 128 rows x 128 B
@@ -185,6 +186,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 8 consecutive FP32 TMEM columns of this warp's 32 lanes.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Shared-memory matrix descriptor (tcgen05): start, leading / stride byte
 // offsets, version 1, layout (0 = no swizzle, 2 = 128-byte swizzle).
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
@@ -240,15 +255,18 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   unsigned char* sBl = base + Ly.bl;
   unsigned char* sR = base + Ly.r;
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + Ly.bars);
+  // X moves in K halves h (boxes kb in [h nkb/nh, (h+1) nkb/nh)): GEMM2's
+  // d-half h reads exactly X's K half h, so the next block's half h loads
+  // while GEMM2's later half and GEMM1's earlier half run.
   uint64_t* bar_b = bars + 0;  // B tile loaded
-  uint64_t* bar_x = bars + 1;  // X tile loaded
-  uint64_t* bar_l = bars + 2;  // GEMM1 done (L ready)
-  uint64_t* bar_r = bars + 3;  // epilogue wrote R (128 arrivals)
-  uint64_t* bar_g = bars + 4;  // GEMM2 done (X, R free)
-  uint64_t* bar_z = bars + 5;  // teardown drain
+  uint64_t* bar_x = bars + 1;  // [2] X K half h loaded
+  uint64_t* bar_l = bars + 3;  // GEMM1 done (L ready)
+  uint64_t* bar_r = bars + 4;  // epilogue wrote R (256 arrivals)
+  uint64_t* bar_g = bars + 5;  // [2] GEMM2 half h done (X K half h free; R free after the last)
+  uint64_t* bar_z = bars + 7;  // teardown drain
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
-  __shared__ double s_red[kEpi][BT / 2];
+  __shared__ double s_red[kEpi][BT / kParts];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t t0 = static_cast<int64_t>(blockIdx.x) * BT;
@@ -259,9 +277,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   if (threadIdx.x == 0) {
     mbar_init(bar_b, 1);
     mbar_init(bar_x, 1);
+    mbar_init(bar_x + 1, 1);
     mbar_init(bar_l, 1);
     mbar_init(bar_r, 32 * kEpi);
     mbar_init(bar_g, 1);
+    mbar_init(bar_g + 1, 1);
     mbar_init(bar_z, 1);
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -288,35 +308,40 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         tma_2d(sBl + kb * kBoxBl, &tmBl, kb * 64, static_cast<int>(t0), bar_b);
       }
       ok = mbar_wait(bar_b, 0, err);
-      int issued = 0;
-      for (int nb = 0; nb < nblocks && ok; ++nb, err) {
-        if (nb > 0 && !(ok = mbar_wait(bar_g, (nb - 1) & 1, err))) break;
-        mbar_expect_tx(bar_x, 2 * nkb * kBoxX);
-        for (int kb = 0; kb < nkb; ++kb) {
-          tma_2d(sXh + kb * kBoxX, &tmXh, kb * 64, nb * BN, bar_x);
-          tma_2d(sXl + kb * kBoxX, &tmXl, kb * 64, nb * BN, bar_x);
+      const int kbh = nkb / nh;  // X boxes per K half
+      auto load_x = [&](int nb, int h) {
+        mbar_expect_tx(bar_x + h, 2 * kbh * kBoxX);
+        for (int kb = h * kbh; kb < (h + 1) * kbh; ++kb) {
+          tma_2d(sXh + kb * kBoxX, &tmXh, kb * 64, nb * BN, bar_x + h);
+          tma_2d(sXl + kb * kBoxX, &tmXl, kb * 64, nb * BN, bar_x + h);
         }
-        if (!(ok = mbar_wait(bar_x, nb & 1, err))) break;
-        tc_fence_after();
-        // GEMM1: L = Xh [Bh | Bt] + Xh Bl + Xl Bh
-        for (int kb = 0; kb < nkb; ++kb)
+      };
+      if (ok)
+        for (int h = 0; h < nh; ++h) load_x(0, h);
+      for (int nb = 0; nb < nblocks && ok; ++nb) {
+        // GEMM1: L = Xh [Bh | Bt] + Xh Bl + Xl Bh, K half by K half as X arrives
+        for (int h = 0; h < nh; ++h) {
+          if (!(ok = mbar_wait(bar_x + h, nb & 1, err))) break;
+          tc_fence_after();
+          for (int kb = h * kbh; kb < (h + 1) * kbh; ++kb)
 #pragma unroll
-          for (int ks = 0; ks < 4; ++ks) {
-            const uint64_t ah = sdesc(su32(sXh + kb * kBoxX) + ks * 32, 16, 1024, 2);
-            const uint64_t al = sdesc(su32(sXl + kb * kBoxX) + ks * 32, 16, 1024, 2);
-            const uint64_t bhz = sdesc(su32(sB1 + kb * kBoxB1) + ks * 32, 16, 1024, 2);
-            const uint64_t bl = sdesc(su32(sBl + kb * kBoxBl) + ks * 32, 16, 1024, 2);
-            mma_f16(tL, ah, bhz, i1_vt, (kb | ks) != 0);
-            mma_f16(tL, ah, bl, i1_v, 1);
-            mma_f16(tL, al, bhz, i1_v, 1);
-          }
+            for (int ks = 0; ks < 4; ++ks) {
+              const uint64_t ah = sdesc(su32(sXh + kb * kBoxX) + ks * 32, 16, 1024, 2);
+              const uint64_t al = sdesc(su32(sXl + kb * kBoxX) + ks * 32, 16, 1024, 2);
+              const uint64_t bhz = sdesc(su32(sB1 + kb * kBoxB1) + ks * 32, 16, 1024, 2);
+              const uint64_t bl = sdesc(su32(sBl + kb * kBoxBl) + ks * 32, 16, 1024, 2);
+              mma_f16(tL, ah, bhz, i1_vt, (kb | ks) != 0);
+              mma_f16(tL, ah, bl, i1_v, 1);
+              mma_f16(tL, al, bhz, i1_v, 1);
+            }
+        }
+        if (!ok) break;
         mma_commit(bar_l);
-        ++issued;
         if (!(ok = mbar_wait(bar_r, nb & 1, err))) break;
         tc_fence_after();
-        if (has_g) {
-          // GEMM2: G_h += Xh^T [Rh | S] + Xh^T Rl + Xl^T Rh  (A MN-major, B MN-major)
-          for (int h = 0; h < nh; ++h)
+        // GEMM2: G_h += Xh^T [Rh | S] + Xh^T Rl + Xl^T Rh  (A MN-major, B MN-major)
+        for (int h = 0; h < nh; ++h) {
+          if (has_g) {
 #pragma unroll
             for (int kn = 0; kn < BN / 16; ++kn) {
               const uint64_t ah = sdesc(su32(sXh + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
@@ -328,8 +353,15 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
               mma_f16(tG + 64 * h, ah, brl, i2_r, 1);
               mma_f16(tG + 64 * h, al, brs, i2_r, 1);
             }
+          }
+          mma_commit(bar_g + h);
         }
-        mma_commit(bar_g);
+        // the next block's X, half h as soon as GEMM2's half h has read it
+        if (nb + 1 < nblocks)
+          for (int h = 0; h < nh; ++h) {
+            if (!(ok = mbar_wait(bar_g + h, nb & 1, err))) break;
+            load_x(nb + 1, h);
+          }
       }
       if (!ok) {
         s_abort = 1;
@@ -338,15 +370,15 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       // drain every MMA this thread issued before TMEM is released
       mma_commit(bar_z);
       if (!mbar_wait(bar_z, 0, err)) atomicExch(err, 1);
-      (void)issued;
     }
     __syncwarp();
   } else {
-    // ---- epilogue: thread = TMEM lane = data row; warp half = column half ----
-    const int quarter = warp & 3, half = warp >> 2;  // columns [16 half, 16 half + 16)
+    // ---- epilogue: thread = TMEM lane = data row; warp part = column block ----
+    const int quarter = warp & 3, part = warp >> 2;  // columns [8 part, 8 part + 8)
     const int row = quarter * 32 + lane;
     const uint32_t lane_off = static_cast<uint32_t>(quarter * 32) << 16;
-    constexpr int BH = BT / 2;
+    constexpr int BH = BT / kParts;
+    static_assert(BH == 8, "one 8-column block of R a thread");
     double lacc[BH];
 #pragma unroll
     for (int t = 0; t < BH; ++t) lacc[t] = 0.0;
@@ -359,10 +391,10 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
-      float v[16], w[16];
-      tmem_ld16(tL + lane_off + BH * half, v);
-      if (has_tangent) tmem_ld16(tL + lane_off + BT + BH * half, w);
-      __half rh[16], rl[16], sh[16];
+      float v[BH], w[BH];
+      tmem_ld8(tL + lane_off + BH * part, v);
+      if (has_tangent) tmem_ld8(tL + lane_off + BT + BH * part, w);
+      __half rh[BH], rl[BH], sh[BH];
 #pragma unroll
       for (int t = 0; t < BH; ++t) {
         const float l = v[t];
@@ -378,27 +410,24 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       }
       if (has_g) {
         const uint32_t roff = static_cast<uint32_t>((row >> 3) * 128 + (row & 7) * 16);
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          const int tb = 2 * half + b;  // 8-column block of this thread's columns
-          *reinterpret_cast<uint4*>(sR + (0 + tb) * kRBlock + roff) = pack8(rh, b);
-          *reinterpret_cast<uint4*>(sR + (4 + tb) * kRBlock + roff) = pack8(sh, b);
-          *reinterpret_cast<uint4*>(sR + (8 + tb) * kRBlock + roff) = pack8(rl, b);
-        }
+        *reinterpret_cast<uint4*>(sR + (0 + part) * kRBlock + roff) = pack8(rh, 0);
+        *reinterpret_cast<uint4*>(sR + (4 + part) * kRBlock + roff) = pack8(sh, 0);
+        *reinterpret_cast<uint4*>(sR + (8 + part) * kRBlock + roff) = pack8(rl, 0);
         fence_async_smem();
       }
       tc_fence_before();
       mbar_arrive(bar_r);
     }
-    if (ok && has_g && mbar_wait(bar_g, (nblocks - 1) & 1, err)) {
+    if (ok && has_g && mbar_wait(bar_g + (nh - 1), (nblocks - 1) & 1, err)) {
       tc_fence_after();
-      // warp half 0 reads the value block, half 1 the tangent block of G
-      for (int h = 0; h < nh; ++h) {
+      // part 2 h + b reads d-half h of G, the value block (b = 0) or the tangent block
+      if (part < 2 * nh) {
+        const int h = part >> 1, b = part & 1;
         float g[32];
-        tmem_ld32(tG + 64 * h + lane_off + BT * half, g);
+        tmem_ld32(tG + 64 * h + lane_off + BT * b, g);
         const int64_t d = 128 * h + row;
         if (d < Dp) {
-          const int64_t cbase = half ? T : 0;
+          const int64_t cbase = b ? T : 0;
 #pragma unroll
           for (int t = 0; t < BT; ++t)
             if (t0 + t < T) G[(cbase + t0 + t) * Dp + d] = g[t];
@@ -412,7 +441,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       const double sum = warp_sum(lacc[t]);
       if (lane == 0) s_red[warp][t] = sum;
     }
-    asm volatile("bar.sync 1, 256;" ::: "memory");
+    asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpi) : "memory");
     if (threadIdx.x < BT && t0 + threadIdx.x < T) {
       const int t = threadIdx.x, hh = t / BH, tt = t % BH;
       double a = 0.0;
