@@ -7,6 +7,7 @@ from types import SimpleNamespace
 
 from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupported,
                    default_handle, load)
+from .adapt import AdaptiveMALASampler, adapt_step_size, dual_average_update
 from .core import (Chain, DensityModel, ParallelMALASampler, ParallelMALAState,
                    ParallelMALATransition, adjoint, fleet_solve, sample, solve,
                    solve_affine_scan_diag, step, tape)
@@ -19,6 +20,6 @@ __all__ = [
     "ArgumentError", "DimensionMismatch", "DeviceError", "Unsupported", "Handle",
     "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
     "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
-    "step", "tape",
+    "step", "tape", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
     "solve_affine_scan_diag", "DEER", "DEERScan",
 ]

@@ -1,0 +1,62 @@
+"""Dual averaging of the step size (the reference's _dual_average_update,
+src/interface.jl:962-984, and AdaptiveMALASampler's validation, :911-933):
+host arithmetic, no GPU."""
+import math
+
+import numpy as np
+import pytest
+
+import pmcmc
+from pmcmc import AdaptiveMALASampler, dual_average_update
+
+
+def _restated(eps0, eps_bar, H_bar, m, logalpha, delta, gamma, t0, kappa):
+    alpha = np.minimum(1.0, np.exp(logalpha))
+    eta = 1.0 / (m + t0)
+    H = (1 - eta) * H_bar + eta * (delta - alpha)
+    le = np.log(10 * eps0) - np.sqrt(m) / gamma * H
+    w = m ** (-kappa)
+    return np.exp(le), np.exp(w * le + (1 - w) * np.log(eps_bar)), H
+
+
+def test_update_matches_the_formula():
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        ad = AdaptiveMALASampler(10 ** rng.uniform(-3, 0), target_accept=rng.uniform(0.2, 0.9),
+                                 gamma=rng.uniform(0.01, 0.2), t0=rng.uniform(1, 20),
+                                 kappa=rng.uniform(0.51, 1.0))
+        args = (ad.epsilon_init, 10 ** rng.uniform(-3, 0), rng.normal(0, 0.1),
+                int(rng.integers(1, 5000)), -abs(rng.normal(0, 2)))
+        got = dual_average_update(*args, ad)
+        ref = _restated(*args, ad.target_accept, ad.gamma, ad.t0, ad.kappa)
+        np.testing.assert_allclose(got, ref, rtol=1e-12)
+
+
+def test_direction_of_the_update():
+    ad = AdaptiveMALASampler(0.1)
+    e_hi = e_lo = (0.1, 0.1, 0.0)
+    for m in range(1, 200):
+        e_hi = dual_average_update(0.1, e_hi[1], e_hi[2], m, 0.0, ad)        # always accepted
+        e_lo = dual_average_update(0.1, e_lo[1], e_lo[2], m, -math.inf, ad)  # never accepted
+    assert e_hi[1] > 0.1 > e_lo[1]
+    # at the target rate H stays 0 and epsilon sits at the prior centre 10 eps0
+    e = dual_average_update(0.1, 0.1, 0.0, 1, math.log(ad.target_accept), ad)
+    assert e[2] == pytest.approx(0.0, abs=1e-15) and e[0] == pytest.approx(1.0)
+
+
+@pytest.mark.parametrize("kw", [dict(epsilon_init=0.0), dict(epsilon_init=0.1, target_accept=1.0),
+                                dict(epsilon_init=0.1, gamma=0.0), dict(epsilon_init=0.1, t0=0.0),
+                                dict(epsilon_init=0.1, kappa=0.5),
+                                dict(epsilon_init=0.1, kappa=1.5)])
+def test_validation_mirrors_the_reference(kw):
+    with pytest.raises(pmcmc.ArgumentError):
+        AdaptiveMALASampler(**kw)
+
+
+def test_adapt_arguments_are_checked():
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(3))
+    s = pmcmc.ParallelMALASampler(0.1, T=8)
+    with pytest.raises(pmcmc.ArgumentError):
+        pmcmc.adapt_step_size(model, s, np.zeros(3), method="newton")
+    with pytest.raises(pmcmc.ArgumentError):
+        pmcmc.adapt_step_size(model, s, np.zeros(3), n_blocks=0)
