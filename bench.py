@@ -130,6 +130,20 @@ def cpu_reference_block(model, sampler, x0, seed, block, nthreads):
     return S, info, dt
 
 
+def cpu_sequential_block(model, sampler, x0, seed, block):
+    """The sequential taped MALA chain (MALA.jl:322-346, 377-411) on one block, one
+    thread, FP64: the trace DEER reproduces."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    tg = model.target
+    otg = O.Target.diag_gauss(tg["prec"], tg["mean"])
+    Xi, u = O.tape(seed, block, model.dim, sampler.T)
+    t0 = time.perf_counter()
+    O.mala_sequential(otg, sampler.epsilon, np.asarray(x0, np.float64), Xi, u)
+    return time.perf_counter() - t0
+
+
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -302,6 +316,26 @@ def run_ours(args):
         traffic = 6754048
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
 
+    # ---- sequential MALA on the device (pmcmc_mala_chains): one chain over the same
+    # block, and a chain a warp on every SM for throughput
+    def chains_rate(n):
+        x0c = x0_dev.repeat(n, 1).contiguous()
+        sd = torch.arange(n, dtype=torch.int64, device=dev) + seed
+        Sc = torch.empty((n, T, D), dtype=torch.float32, device=dev)
+        p = sampler.params()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        L.check(lib.pmcmc_mala_chains(h.ptr, tgt, C.byref(p), n, x0c.data_ptr(), sd.data_ptr(),
+                                      1000, Sc.data_ptr(), None, None, L.MEM_DEVICE), h.ptr,
+                "mala_chains")
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return n * T / (e0.elapsed_time(e1) / 1e3)
+
+    chains_rate(1)
+    seq_one = chains_rate(1)
+    seq_many = chains_rate(8 * torch.cuda.get_device_properties(dev).multi_processor_count)
+
     # ---- end to end through the public API with host buffers: one sample() call of
     # E2E_BLOCKS blocks per step (x0 in, the chain's values, logp and accept flags out;
     # block b's copy-out overlaps block b + 1's solve), and of one block for reference
@@ -333,6 +367,10 @@ def run_ours(args):
                "sample": f"one full block (T={T}): FP64 C restatement of the reference CPU DEER "
                          f"(per-t :diag, D JVPs per column, doubling scan), "
                          f"{cinfo['iters']} Newton iterations, OpenMP"}
+        sdt = cpu_sequential_block(model, sampler, x0, seed, 0)
+        cpu["sequential_mala"] = {"value": T / sdt, "unit": "samples/s", "cores": 1,
+                                  "sample": f"the sequential taped MALA chain over the same "
+                                            f"block (T={T}), FP64 C, one thread"}
 
     if pg:
         pg.barrier()
@@ -353,6 +391,11 @@ def run_ours(args):
                             f"arrays, wall clock",
                     "one_block": {"value": e2e_one, "step": "pmcmc.sample(N=T)",
                                   "d2h_bytes_per_step": 4 * D * T + 4 * T + T}},
+            "gpu_sequential_mala": {"one_chain": seq_one,
+                                    "one_chain_speedup_of_deer": value / world / seq_one,
+                                    "chains_8_per_sm": seq_many, "unit": "samples/s",
+                                    "note": "independent taped MALA chains, one warp each "
+                                            "(pmcmc_mala_chains), same block and tape"},
             "plain_gpu": {"value": plain_value, "unit": "samples/s",
                           "newton_iters_mean": statistics.mean(i.iters for i in pinfos),
                           "speedup_fused_over_plain": value / world / plain_value},

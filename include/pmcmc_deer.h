@@ -284,6 +284,20 @@ typedef struct {
 int pmcmc_set_profiling(pmcmc_handle* h, int32_t on);
 int pmcmc_get_profile(pmcmc_handle* h, pmcmc_profile* out, int32_t reset);
 
+/* pmcmc_mala_chains (no counterpart entry point in the reference, which runs
+ * such chains one by one on the CPU, src/MALA/MALA.jl:322-346, 377-411): n independent
+ * sequential MALA chains of p->T steps each, one warp a chain.  Chain c starts
+ * at x0[c*D .. c*D+D) and uses the tape of (seeds[c], block), the tape a DEER
+ * solve with that seed and block uses, so its trajectory is the one DEER
+ * converges to.  Outputs: S_out n x T x D (step t of chain c at
+ * (c*T + t)*D), logp_out n x T and accept_out n x T (either may be NULL).
+ * Element type per p->dtype; Gaussian targets only (others return
+ * PMCMC_ERR_UNSUPPORTED); p is validated as for a solve, and only its
+ * epsilon, T and dtype are used. */
+int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                      int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
+                      void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem);
+
 /* ---- bound check of the device waits (no counterpart in the reference, whose
  * device code never waits on another block) ------------------------------------
  * Runs one of the library's bounded waits on a flag that nothing sets: the

@@ -1804,6 +1804,71 @@ int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T,
   return PMCMC_OK;
 }
 
+int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                      int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
+                      void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem) {
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0 || !seeds || !S_out)
+    return fail(h, PMCMC_ERR_ARGUMENT, "x0, seeds and S_out must not be NULL");
+  if (n < 1) return fail(h, PMCMC_ERR_ARGUMENT, "the number of chains must be >= 1");
+  if (mem != PMCMC_MEM_HOST && mem != PMCMC_MEM_DEVICE)
+    return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
+  if (tg->kind == kLogistic)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "sequential chains are built for Gaussian targets");
+  DeviceGuard guard(h->device);
+  const bool f64 = p->dtype == PMCMC_F64;
+  const size_t es = f64 ? 8 : 4;
+  const int64_t D = tg->D, T = p->T;
+  if (mala_chains_smem(f64, tg->Dp, tg->kind == kDenseGauss) > 200 * 1024)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "dimension %lld too large for the chain kernel",
+                (long long)D);
+  DevParams P{};
+  P.D = D;
+  P.Dp = tg->Dp;
+  P.T = T;
+  P.W = T;
+  P.eps = p->epsilon;
+  P.sqrt2eps = std::sqrt(2 * p->epsilon);
+  P.inv4eps = 1.0 / (4 * p->epsilon);
+  P.inv2eps = 1.0 / (2 * p->epsilon);
+  P.block = block;
+  P.tkind = tg->kind;
+  P.mean_d = tg->mean_d;
+  P.prec_d = tg->prec_d;
+  P.mean_f = tg->mean_f;
+  P.prec_f = tg->prec_f;
+  const void* dx0 = x0;
+  const uint64_t* dseeds = seeds;
+  void *dS = S_out, *dlp = logp_out;
+  uint8_t* dacc = accept_out;
+  const size_t bx = es * n * D, bs = 8 * static_cast<size_t>(n), bS = es * n * T * D,
+               blp = logp_out ? es * n * T : 0, bacc = accept_out ? n * T : 0;
+  if (mem == PMCMC_MEM_HOST) {
+    auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+    rc = ensure_ws(h, a(bx) + a(bs) + a(bS) + a(blp) + a(bacc));
+    if (rc) return rc;
+    unsigned char* w = h->ws;
+    dx0 = w;
+    dseeds = reinterpret_cast<const uint64_t*>(w + a(bx));
+    dS = w + a(bx) + a(bs);
+    dlp = logp_out ? w + a(bx) + a(bs) + a(bS) : nullptr;
+    dacc = accept_out ? w + a(bx) + a(bs) + a(bS) + a(blp) : nullptr;
+    CK(cudaMemcpyAsync(const_cast<void*>(dx0), x0, bx, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(const_cast<uint64_t*>(dseeds), seeds, bs, cudaMemcpyHostToDevice,
+                       h->stream));
+  }
+  CK(launch_mala_chains(h->stream, f64, tg->kind, P, n, dx0, dseeds, dS, dlp, dacc));
+  if (mem == PMCMC_MEM_HOST) {
+    CK(cudaMemcpyAsync(S_out, dS, bS, cudaMemcpyDeviceToHost, h->stream));
+    if (logp_out) CK(cudaMemcpyAsync(logp_out, dlp, blp, cudaMemcpyDeviceToHost, h->stream));
+    if (accept_out)
+      CK(cudaMemcpyAsync(accept_out, dacc, bacc, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PMCMC_OK;
+}
+
 int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q) {
   if (!t || !lam) return PMCMC_ERR_ARGUMENT;
   const int rc = ensure_eigen(t->h, t);

@@ -40,6 +40,14 @@ SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D);
 SweepKernels logistic_sweep_kernels(bool f64, int64_t D);
 SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);
 
+// Independent sequential MALA chains, one warp a chain (mala_chains.cu): chain c
+// from x0[c * D ..] with the tape of (seeds[c], P.block); S is nchains x T x D.
+struct DevParams;
+size_t mala_chains_smem(bool f64, int64_t Dp, bool dense);
+cudaError_t launch_mala_chains(cudaStream_t s, bool f64, int tk, const DevParams& P,
+                               int64_t nchains, const void* x0, const uint64_t* seeds, void* S,
+                               void* logp, uint8_t* acc);
+
 // Tape materialisation (tape.cu).
 cudaError_t launch_tape(cudaStream_t s, int64_t D, int64_t T, uint64_t seed, uint64_t block,
                         float* Xi, float* u);

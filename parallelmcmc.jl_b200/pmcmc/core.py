@@ -385,6 +385,33 @@ def solve(model: DensityModel, sampler: ParallelMALASampler, s0, *, seed: int = 
     return Sv, info.as_dict()
 
 
+# --------------------------------------------------------------------------- sequential chains
+def mala_chains(model: DensityModel, sampler: ParallelMALASampler, x0s, seeds, *,
+                block: int = 0, handle: Optional[L.Handle] = None, device: int = 0):
+    """n independent sequential MALA chains of sampler.T steps on the device,
+    one warp a chain (the reference's MALASampler chains run side by side,
+    MALA.jl:322-346, 377-411).  x0s: (n, D); seeds: (n,).  Chain c uses the
+    tape of (seeds[c], block), the tape DEER uses for that seed and block.
+    Returns S (n, T, D), logp (n, T) and accept flags (n, T)."""
+    h = handle or L.default_handle(device)
+    tgt = model.device_target(h)
+    x = np.ascontiguousarray(np.asarray(x0s, dtype=sampler.dtype).reshape(-1, model.dim))
+    n = x.shape[0]
+    sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(-1))
+    if sd.size != n:
+        raise DimensionMismatch("one seed per chain")
+    T = int(sampler.T)
+    S = np.empty((n, T, model.dim), sampler.dtype)
+    lp = np.empty((n, T), sampler.dtype)
+    acc = np.empty((n, T), np.uint8)
+    p = sampler.params()
+    rc = L.load().pmcmc_mala_chains(h.ptr, tgt, C.byref(p), n, x.ctypes.data, sd.ctypes.data,
+                                    int(block), S.ctypes.data, lp.ctypes.data, acc.ctypes.data,
+                                    L.MEM_HOST)
+    L.check(rc, h.ptr, "mala_chains")
+    return S, lp, acc.astype(bool)
+
+
 # --------------------------------------------------------------------------- adjoint
 def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objective: str = "esjd",
             seed: int = 0, block: int = 0, handle: Optional[L.Handle] = None, device: int = 0):
