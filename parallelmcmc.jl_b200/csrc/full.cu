@@ -357,10 +357,12 @@ __global__ void __launch_bounds__(544)
 }
 
 // ---------------------------------------------------------------------------
-// carry: din_0 = 0, din_{c+1} = Phi'_c din_c + beta'_c (one CTA).  Chunk maps
-// stream through an NST-stage cp.async ring; a step is one mat-vec, thread
-// (part, row) summing KC terms from the column-major map (conflict-free),
-// partial sums combined through shared memory.
+// carry: din_0 = 0, din_{c+1} = Phi'_c din_c + beta'_c (one CTA).  Thread
+// (part, row) sums KC terms of row `row` (the map is column-major, so the
+// threads of a part read consecutive rows: coalesced), partial sums combined
+// through shared memory.  Each thread keeps its KC map entries for the next
+// two chunks in registers, loaded from L2 two steps ahead (a three-slot ring),
+// so a step waits on no copy.
 // ---------------------------------------------------------------------------
 template <int DQ, int NST>
 __global__ void __launch_bounds__(256)
@@ -368,64 +370,68 @@ __global__ void __launch_bounds__(256)
                       DevState* __restrict__ st, cudaGraphConditionalHandle, int use_cond) {
   constexpr int PARTS = DQ >= 128 ? 2 : 4;
   constexpr int KC = DQ / PARTS;
-  constexpr int STAGE = DQ * DQ + DQ;  // floats per stage: Phi then beta
+  static_assert(PARTS * DQ <= 256, "one thread a (part, row)");
   __shared__ DevParams P;
   __shared__ FullArgs F;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float vec[2][DQ];
+  __shared__ float pbuf[PARTS][DQ];
   load_struct(Fg, F);
   __syncthreads();
   load_params(F.Pe, P);
   if (sweep_done(st, use_cond, P.maxiter)) return;
   const int tid = threadIdx.x;
   const int nch = F.nchunks;
-  float* stage = reinterpret_cast<float*>(smem_raw);
-  float* vec = stage + NST * STAGE;  // 2 x DQ
-  float* pbuf = vec + 2 * DQ;        // PARTS x DQ
-  for (int i = tid; i < 2 * DQ; i += blockDim.x) vec[i] = 0.f;
-  for (int i = tid; i < DQ; i += blockDim.x) F.din[i] = 0.f;
-  auto issue = [&](int c) {
-    if (c < nch - 1) {
-      float* dst = stage + (c % NST) * STAGE;
-      const float* sp = F.Phi + static_cast<size_t>(c) * DQ * DQ;
-      const float* sb = F.beta + static_cast<size_t>(c) * DQ;
-      constexpr int n4p = DQ * DQ / 4, n4b = DQ / 4;
-      for (int i = tid; i < n4p + n4b; i += blockDim.x) {
-        if (i < n4p) cp_async16(dst + 4 * i, sp + 4 * i);
-        else cp_async16(dst + DQ * DQ + 4 * (i - n4p), sb + 4 * (i - n4p));
-      }
-    }
-    cp_async_commit();
-  };
-#pragma unroll
-  for (int c = 0; c < NST - 1; ++c) issue(c);
   const int row = tid % DQ, part = tid / DQ;
   const bool worker = part < PARTS;
   const int k0 = part * KC;
-  for (int c = 0; c < nch - 1; ++c) {
-    cp_async_wait<NST - 2>();
-    __syncthreads();  // chunk c landed; step c-1 (and its stage) is finished
-    issue(c + NST - 1);
+  for (int i = tid; i < 2 * DQ; i += blockDim.x) (&vec[0][0])[i] = 0.f;
+  for (int i = tid; i < DQ; i += blockDim.x) F.din[i] = 0.f;
+  float m[3][KC];
+  float bt[3] = {0.f, 0.f, 0.f};
+  auto fetch = [&](int c, float (&dst)[KC], float& b) {
+    if (c < nch - 1) {
+      if (worker) {
+        const float* Ph = F.Phi + static_cast<size_t>(c) * DQ * DQ + static_cast<size_t>(k0) * DQ + row;
+#pragma unroll
+        for (int k = 0; k < KC; ++k) dst[k] = __ldcg(Ph + static_cast<size_t>(k) * DQ);
+      }
+      if (tid < DQ) b = __ldcg(F.beta + static_cast<size_t>(c) * DQ + tid);
+    }
+  };
+  auto step = [&](int c, const float (&cur)[KC], float b) {
     if (worker) {
-      const float* Ph = stage + (c % NST) * STAGE + k0 * DQ + row;
-      const float* x = vec + (c & 1) * DQ + k0;
+      const float* x = vec[c & 1] + k0;
       float a0 = 0.f, a1 = 0.f;
 #pragma unroll
       for (int k = 0; k < KC; k += 2) {
-        a0 = fmaf(Ph[k * DQ], x[k], a0);
-        a1 = fmaf(Ph[(k + 1) * DQ], x[k + 1], a1);
+        a0 = fmaf(cur[k], x[k], a0);
+        a1 = fmaf(cur[k + 1], x[k + 1], a1);
       }
-      pbuf[part * DQ + row] = a0 + a1;
+      pbuf[part][row] = a0 + a1;
     }
     __syncthreads();
     if (tid < DQ) {
-      float y = stage[(c % NST) * STAGE + DQ * DQ + tid];
+      float y = b;
 #pragma unroll
-      for (int p = 0; p < PARTS; ++p) y += pbuf[p * DQ + tid];
-      vec[((c + 1) & 1) * DQ + tid] = y;
+      for (int p = 0; p < PARTS; ++p) y += pbuf[p][tid];
+      vec[(c + 1) & 1][tid] = y;
       F.din[static_cast<size_t>(c + 1) * DQ + tid] = y;
     }
+    __syncthreads();
+  };
+  __syncthreads();
+  fetch(0, m[0], bt[0]);
+  fetch(1, m[1], bt[1]);
+  for (int c = 0; c < nch - 1; c += 3) {
+    fetch(c + 2, m[2], bt[2]);
+    step(c, m[0], bt[0]);
+    if (c + 1 >= nch - 1) break;
+    fetch(c + 3, m[0], bt[0]);
+    step(c + 1, m[1], bt[1]);
+    if (c + 2 >= nch - 1) break;
+    fetch(c + 4, m[1], bt[1]);
+    step(c + 2, m[2], bt[2]);
   }
-  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -861,11 +867,13 @@ bool full_plan(int64_t Dp, int64_t T, int tkind, int num_sms, int chunks_overrid
   int Lmax = 1;
   while (Lmax < 4096 && chunk_smem(Dq, Lmax + 1) <= budget && apply_smem(Dq, Dp, Lmax + 1) <= budget)
     ++Lmax;
-  // the sequential depth of a sweep is ~L chunk steps + nchunks carry steps +
-  // L replay steps of similar latency: about sqrt(T / 2) chunks balances them
+  // the sequential depth of a sweep is ~L chunk steps + L replay steps +
+  // nchunks carry steps, a carry step about a quarter of the cost of the other
+  // two together: about sqrt(2 T) chunks balances them (128 at T = 8192:
+  // 121 us a sweep against 139 us at 64 chunks, D = 64)
   int nch = chunks_override > 0
                 ? chunks_override
-                : std::min(num_sms, static_cast<int>(std::sqrt(0.5 * static_cast<double>(T)) + 0.5));
+                : std::min(num_sms, static_cast<int>(std::sqrt(2.0 * static_cast<double>(T)) + 0.5));
   nch = std::max(1, nch);
   int64_t L = (T + nch - 1) / nch;
   if (L > Lmax) L = Lmax;
@@ -875,7 +883,9 @@ bool full_plan(int64_t Dp, int64_t T, int tkind, int num_sms, int chunks_overrid
   fp->smem_apply = apply_smem(Dq, Dp, fp->L);
   const int nst = carry_stages(Dq);
   const int parts = Dq >= 128 ? 2 : 4;
-  fp->smem_carry = sizeof(float) * (static_cast<size_t>(nst) * (Dq * Dq + Dq) + 2 * Dq + parts * Dq);
+  fp->smem_carry = 0;  // static shared memory only
+  (void)nst;
+  (void)parts;
   fp->smem_eval = plan_sweep_smem<float>(Dq, 1, false).total;
   fp->eval_grid =
       static_cast<int>(std::min<int64_t>((T + kWarps - 1) / kWarps, int64_t(num_sms) * 4));
