@@ -325,7 +325,7 @@ struct SolveLayout {
   size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
   size_t xi, logu;
   size_t tcws, Gtc;  // tensor-core logistic path
-  size_t fU, fV, fR, facc, fPhi, fbeta, fdin, eS0, eS1, exi, ex0;  // :full mode
+  size_t fU, fV, fR, facc, fPhi, fbeta, fdin, fpart, eS0, eS1, exi, ex0;  // :full mode
   size_t alam, acterm, aarev, adirect, ascr, aout;                 // adjoint
   size_t out2_S, out2_lp, out2_acc;  // second output slot of the host-output pipeline
   size_t part;                       // per-CTA partial reductions of the persistent solve
@@ -399,6 +399,7 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
     L.fPhi = take(4 * static_cast<size_t>(fp->nchunks) * Dq * Dq);
     L.fbeta = take(4 * static_cast<size_t>(fp->nchunks) * Dq);
     L.fdin = take(4 * static_cast<size_t>(fp->nchunks) * Dq);
+    L.fpart = take(16 * static_cast<size_t>(fp->nchunks));
   }
   if (adjoint) {
     L.alam = take(4 * T * Dp);
@@ -1217,6 +1218,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     F.Phi = reinterpret_cast<float*>(ws + L.fPhi);
     F.beta = reinterpret_cast<float*>(ws + L.fbeta);
     F.din = reinterpret_cast<float*>(ws + L.fdin);
+    F.part = reinterpret_cast<double*>(ws + L.fpart);
     F.L = fplan.L;
     F.nchunks = fplan.nchunks;
     F.rot = dense ? 1 : 0;

@@ -505,22 +505,39 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int e = 0; e < 4; ++e) lc[e] = 4 * lane + e < D ? 1.f - eps * l4[e] : 0.f;
     }
-    for (int s = 0; s < nt; ++s) {
-      float u[4] = {0.f, 0.f, 0.f, 0.f}, v[4] = {0.f, 0.f, 0.f, 0.f}, r[4] = {0.f, 0.f, 0.f, 0.f};
+    // step s's u', v', r' and accept flag are loaded during step s - 1
+    float u[4] = {0.f, 0.f, 0.f, 0.f}, v[4] = {0.f, 0.f, 0.f, 0.f}, r[4] = {0.f, 0.f, 0.f, 0.f};
+    bool a = false;
+    if (nt > 0) {
       if (in) {
-        load4(Us + s * DQ + 4 * lane, u);
-        load4(Vs + s * DQ + 4 * lane, v);
-        load4(Rs + s * DQ + 4 * lane, r);
+        load4(Us + 4 * lane, u);
+        load4(Vs + 4 * lane, v);
+        load4(Rs + 4 * lane, r);
+      }
+      a = as[0] != 0;
+    }
+    for (int s = 0; s < nt; ++s) {
+      float un[4] = {0.f, 0.f, 0.f, 0.f}, vn[4] = {0.f, 0.f, 0.f, 0.f}, rn[4] = {0.f, 0.f, 0.f, 0.f};
+      bool an = false;
+      if (s + 1 < nt) {
+        if (in) {
+          load4(Us + (s + 1) * DQ + 4 * lane, un);
+          load4(Vs + (s + 1) * DQ + 4 * lane, vn);
+          load4(Rs + (s + 1) * DQ + 4 * lane, rn);
+        }
+        an = as[s + 1] != 0;
       }
       const float dot = warp_sum((v[0] * d[0] + v[1] * d[1]) + (v[2] * d[2] + v[3] * d[3]));
-      if (as[s]) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) d[e] = fmaf(u[e], dot, lc[e] * d[e]) + r[e];
-      } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) d[e] = fmaf(u[e], dot, d[e]) + r[e];
-      }
+      for (int e = 0; e < 4; ++e) d[e] = fmaf(u[e], dot, (a ? lc[e] : 1.f) * d[e]) + r[e];
       if (in) store4(Rs + s * DQ + 4 * lane, d);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        u[e] = un[e];
+        v[e] = vn[e];
+        r[e] = rn[e];
+      }
+      a = an;
     }
   }
   cp_async_wait<0>();
@@ -530,7 +547,7 @@ __global__ void __launch_bounds__(kThreads)
   const float* x0 = static_cast<const float*>(P.x0);
   const float* x0e = static_cast<const float*>(Pe.x0);
   const float dmp = static_cast<float>(P.damping);
-  double dm = 0.0, smx = 0.0;
+  float dm = 0.f, smx = 0.f;  // maxima are exact in FP32
   bool bad = false;
   for (int tile = warp; 8 * tile < nt; tile += kWarps) {
     const int c0 = 8 * tile;
@@ -548,8 +565,8 @@ __global__ void __launch_bounds__(kThreads)
         for (int e = 0; e < 4; ++e) {
           if (4 * lane + e < D) {
             n[e] = fmaf(dmp, acc[c][e], o[e]);
-            dm = fmax(dm, static_cast<double>(fabsf(n[e] - o[e])));
-            smx = fmax(smx, static_cast<double>(fabsf(n[e])));
+            dm = fmaxf(dm, fabsf(n[e] - o[e]));
+            smx = fmaxf(smx, fabsf(n[e]));
             bad |= !isfinite(n[e]);
           } else {
             n[e] = 0.f;
@@ -571,29 +588,45 @@ __global__ void __launch_bounds__(kThreads)
   smx = warp_max(smx);
   bad = __any_sync(0xffffffffu, bad);
   if (lane == 0) {
-    r_dm[warp] = dm;
-    r_sm[warp] = smx;
+    r_dm[warp] = static_cast<double>(dm);
+    r_sm[warp] = static_cast<double>(smx);
     if (bad) s_bad = 1;
   }
   __syncthreads();
   if (tid == 0) {
+    // this CTA's maxima into its own slot (no contended atomics)
     for (int w = 1; w < kWarps; ++w) {
       r_dm[0] = fmax(r_dm[0], r_dm[w]);
       r_sm[0] = fmax(r_sm[0], r_sm[w]);
     }
-    if (r_dm[0] > 0) atomicMax(&st->dmax_bits, dbits(r_dm[0]));
-    if (r_sm[0] > 0) atomicMax(&st->smax_bits, dbits(r_sm[0]));
+    F.part[2 * blockIdx.x] = r_dm[0];
+    F.part[2 * blockIdx.x + 1] = r_sm[0];
     if (s_bad) atomicCAS(&st->status, 0, static_cast<int>(kStNonfinite));
     __threadfence();
     const unsigned prev = atomicAdd(&st->done_counter, 1u);
     s_last = prev == gridDim.x - 1;
   }
   __syncthreads();
-  if (!s_last || tid != 0) return;
-  // last CTA: convergence test (DEER.jl:567-578) and loop control
+  if (!s_last) return;
+  // last CTA: reduce every CTA's slot, the convergence test (DEER.jl:567-578)
+  // and loop control
   __threadfence();
-  const double dmax = bitsd(atomicAdd(&st->dmax_bits, 0ull));
-  const double smax = bitsd(atomicAdd(&st->smax_bits, 0ull));
+  double pd = 0.0, ps = 0.0;
+  for (int i = tid; i < static_cast<int>(gridDim.x); i += blockDim.x) {
+    pd = fmax(pd, __ldcg(F.part + 2 * i));
+    ps = fmax(ps, __ldcg(F.part + 2 * i + 1));
+  }
+  pd = warp_max(pd);
+  ps = warp_max(ps);
+  __syncthreads();
+  if (lane == 0) {
+    r_dm[warp] = pd;
+    r_sm[warp] = ps;
+  }
+  __syncthreads();
+  if (tid != 0) return;
+  double dmax = 0.0, smax = 0.0;
+  for (int w = 0; w < kWarps; ++w) dmax = fmax(dmax, r_dm[w]), smax = fmax(smax, r_sm[w]);
   const double metric = dmax / (P.tol_abs + P.tol_rel * smax);
   const int status = atomicAdd(&st->status, 0);
   const int iter = st->iter;

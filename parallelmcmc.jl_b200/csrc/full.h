@@ -30,6 +30,7 @@ struct FullArgs {
   float* Phi;           // nchunks x Dq x Dq chunk maps (column-major)
   float* beta;          // nchunks x Dq      chunk offsets
   float* din;           // nchunks x Dq      primed update entering each chunk
+  double* part;         // nchunks x 2       each apply CTA's max|dS|, max|S|
   int32_t L, nchunks;
   int32_t rot, Dq;
   // adjoint
