@@ -298,6 +298,18 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_p
                       int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
                       void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem);
 
+/* pmcmc_autotune (no counterpart in the reference): times the candidate
+ * shapes of the kernels that would solve (t, p) on x0 and keeps the fastest
+ * for every later solve of the same shape (target kind, Jacobian, precision, D,
+ * T), process-wide.  Candidates: CTAs a SM of the persistent solve (1..4, as
+ * fit), or the :full chunk count (about sqrt(f T), f = 1/2, 1, 2, 4).  Each
+ * candidate solves tape block 0 of `seed` three times (the first warms up).
+ * *choice gets the kept value (0 when the path has nothing to tune) and
+ * *best_ms its time.  Allocates and frees its own scratch. */
+int pmcmc_autotune(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
+                   const void* x0, uint64_t seed, int32_t mem, int32_t* choice,
+                   double* best_ms);
+
 /* ---- bound check of the device waits (no counterpart in the reference, whose
  * device code never waits on another block) ------------------------------------
  * Runs one of the library's bounded waits on a flag that nothing sets: the

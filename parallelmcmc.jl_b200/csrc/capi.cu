@@ -14,6 +14,7 @@
 #include <cstring>
 #include <atomic>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -84,6 +85,9 @@ struct pmcmc_handle {
   cudaGraphConditionalHandle cond_full = 0;
   unsigned char gkey_full[192] = {};
   int full_chunks_override = 0;
+  // candidate shapes while pmcmc_autotune times them (0: none)
+  int tune_per_sm = 0;
+  int tune_full_chunks = 0;
   SliceState slice;
   std::vector<pmcmc_handle*> fleet;  // worker handles of pmcmc_fleet_solve (own streams)
   // host-output pipeline of multi-block solves: block b's device-to-host copy
@@ -293,12 +297,51 @@ TilePlan choose_tile(pmcmc_handle* h, const SweepKernels& k, bool f64, int64_t D
   return tp;
 }
 
-// Columns per CTA of the persistent solve: the most CTAs a SM whose tiles all
-// fit co-resident (one cooperative launch), TT = ceil(T / (CTAs a SM x SMs));
-// 0 when none fits.
+// Shapes chosen by pmcmc_autotune, process-wide, keyed by problem shape:
+// what = 0: CTAs a SM of the persistent solve; what = 1: :full chunk count.
+struct TuneKey {
+  int what, kind, jac, f64;
+  int64_t D, T;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(what, kind, jac, f64, D, T) < std::tie(o.what, o.kind, o.jac, o.f64, o.D, o.T);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+
+int tune_get(const TuneKey& k) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(k);
+  return it == g_tune.end() ? 0 : it->second;
+}
+void tune_put(const TuneKey& k, int v) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[k] = v;
+}
+
+// TT for `per_sm` co-resident CTAs a SM of the persistent solve, 0 if they do not fit.
+int persist_tile_for(const void* fn, bool f64, int64_t Dp, int64_t T, bool dense, int per_sm,
+                     int num_sms) {
+  const int64_t TT = (T + int64_t(per_sm) * num_sms - 1) / (int64_t(per_sm) * num_sms);
+  if (TT > 256) return 0;
+  const size_t smem = persist_smem(f64, Dp, static_cast<int>(TT), dense).total;
+  if (smem > 200 * 1024) return 0;
+  const int nb = max_active_blocks(fn, smem);
+  return nb >= per_sm ? static_cast<int>(TT) : 0;
+}
+
+// Columns per CTA of the persistent solve: the autotuned CTAs a SM for this
+// shape when there is one, else the most CTAs a SM whose tiles all fit
+// co-resident (one cooperative launch), TT = ceil(T / (CTAs a SM x SMs)); 0
+// when none fits.
 int choose_persist_tile(pmcmc_handle* h, const void* fn, bool f64, int64_t Dp, int64_t T,
-                        bool dense) {
+                        bool dense, const TuneKey& key) {
   if (!fn || h->no_coop || h->tile_override > 0) return 0;
+  if (h->tune_per_sm > 0) return persist_tile_for(fn, f64, Dp, T, dense, h->tune_per_sm, h->num_sms);
+  if (const int tuned = tune_get(key)) {
+    const int TT = persist_tile_for(fn, f64, Dp, T, dense, tuned, h->num_sms);
+    if (TT > 0) return TT;
+  }
   for (int per_sm = 8; per_sm >= 1; --per_sm) {
     const int64_t TT = (T + int64_t(per_sm) * h->num_sms - 1) / (int64_t(per_sm) * h->num_sms);
     if (TT > 256) break;
@@ -489,9 +532,9 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
               size_t smem_sweep, size_t smem_fin, int fin_grid, int init_grid) {
   const void* sweep_fn = coop ? k.sweep_coop : k.sweep;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
-  if (smem_sweep > 48 * 1024)
+  if (smem_sweep > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(sweep_fn), smem_sweep));
-  if (smem_fin > 48 * 1024)
+  if (smem_fin > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem_fin));
   if (!h->force_eager && !h->profiling) {
     GraphKey key;
@@ -584,7 +627,7 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
-  if (smem_fin > 48 * 1024) {
+  if (smem_fin > 0) {
     CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem_fin));
     CK(raise_smem_limit(reinterpret_cast<const void*>(k.eval), smem_fin));
   }
@@ -650,7 +693,7 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
-  if (smem_sweep > 48 * 1024)
+  if (smem_sweep > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(coop ? k.sweep_coop : k.sweep), smem_sweep));
   if (!h->cublas) {
     if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
@@ -984,7 +1027,7 @@ int run_full(pmcmc_handle* h, const SweepKernels& k, const FullPlan& fp, const D
     const size_t sm[6] = {fp.smem_eval, fp.smem_chunk, fp.smem_carry, fp.smem_apply, smem_fin,
                           fp.smem_rotate};
     for (int i = 0; i < 6; ++i)
-      if (sm[i] > 48 * 1024)
+      if (sm[i] > 0)
         CK(raise_smem_limit(reinterpret_cast<const void*>(fns[i]), sm[i]));
   }
   if (!h->force_eager && !h->profiling) {
@@ -1105,7 +1148,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     if (f64) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full is built for FP32 state");
     if (plain) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full has no plain path");
     if (W < T) return fail(h, PMCMC_ERR_UNSUPPORTED, ":full has no sliding window");
-    if (!full_plan(Dp, T, tg->kind, h->num_sms, h->full_chunks_override, &fplan))
+    const int nch = h->full_chunks_override > 0 ? h->full_chunks_override
+                    : h->tune_full_chunks > 0   ? h->tune_full_chunks
+                                                : tune_get(TuneKey{1, tg->kind, p->jacobian, 0, D, T});
+    if (!full_plan(Dp, T, tg->kind, h->num_sms, nch, &fplan))
       return fail(h, PMCMC_ERR_UNSUPPORTED, ":full is built for D <= 128, got %lld",
                   (long long)D);
     rc = ensure_eigen(h, const_cast<pmcmc_target*>(tg));
@@ -1115,7 +1161,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
                                   : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
   // whole solve in one cooperative launch when every tile is co-resident
   const int TTp = (!plain && !logistic && !full && W == T && !h->force_eager && !h->no_persist)
-                      ? choose_persist_tile(h, k.persist, f64, Dp, T, dense)
+                      ? choose_persist_tile(h, k.persist, f64, Dp, T, dense,
+                                            TuneKey{0, tg->kind, p->jacobian, f64, D, T})
                       : 0;
   const bool persist = TTp > 0;
   const TilePlan tp = full      ? TilePlan{}
@@ -1670,6 +1717,92 @@ int pmcmc_tape(pmcmc_handle* h, int64_t D, int64_t T, uint64_t seed, uint64_t bl
   return PMCMC_OK;
 }
 
+int pmcmc_autotune(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                   const void* x0, uint64_t seed, int32_t mem, int32_t* choice,
+                   double* best_ms) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0) return fail(h, PMCMC_ERR_ARGUMENT, "x0 must not be NULL");
+  if (mem != PMCMC_MEM_HOST && mem != PMCMC_MEM_DEVICE)
+    return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
+  DeviceGuard guard(h->device);
+  const bool f64 = p->dtype == PMCMC_F64;
+  const size_t es = f64 ? 8 : 4;
+  const int64_t D = tg->D, T = p->T;
+  const bool full = p->jacobian == PMCMC_JAC_FULL;
+  const bool windowed = p->window > 0 && p->window < T;
+  std::vector<int> cands;
+  TuneKey key{};
+  if (full) {
+    key = TuneKey{1, tg->kind, p->jacobian, 0, D, T};
+    for (double f : {0.5, 1.0, 2.0, 4.0}) {
+      const int n = std::max(1, std::min(h->num_sms, static_cast<int>(std::sqrt(f * T) + 0.5)));
+      if (std::find(cands.begin(), cands.end(), n) == cands.end()) cands.push_back(n);
+    }
+  } else if (p->exec != PMCMC_EXEC_PLAIN && tg->kind != kLogistic && !windowed &&
+             !h->force_eager && !h->no_persist && !h->no_coop && h->tile_override == 0) {
+    key = TuneKey{0, tg->kind, p->jacobian, f64, D, T};
+    const SweepKernels k = gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
+    for (int per_sm = 1; per_sm <= 4; ++per_sm)
+      if (persist_tile_for(k.persist, f64, tg->Dp, T, tg->kind == kDenseGauss, per_sm,
+                           h->num_sms) > 0)
+        cands.push_back(per_sm);
+  }
+  if (choice) *choice = cands.empty() ? 0 : cands.front();
+  if (best_ms) *best_ms = 0.0;
+  if (cands.size() < 2) return PMCMC_OK;  // nothing to choose between
+
+  struct Scratch {
+    void* buf = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    pmcmc_handle* h = nullptr;
+    ~Scratch() {
+      if (h) h->tune_per_sm = h->tune_full_chunks = 0;
+      cudaFree(buf);
+      for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    }
+  } sc;
+  sc.h = h;
+  const size_t bx = (es * D + 255) & ~size_t(255), bS = (es * T * D + 255) & ~size_t(255),
+               blp = (es * T + 255) & ~size_t(255);
+  CK(cudaMalloc(&sc.buf, bx + bS + blp + static_cast<size_t>(T)));
+  CK(cudaEventCreate(&sc.ev[0]));
+  CK(cudaEventCreate(&sc.ev[1]));
+  unsigned char* b = static_cast<unsigned char*>(sc.buf);
+  CK(cudaMemcpyAsync(b, x0, es * D,
+                     mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     h->stream));
+  int best = cands.front();
+  double best_t = INFINITY;
+  for (const int c : cands) {
+    if (full) h->tune_full_chunks = c;
+    else h->tune_per_sm = c;
+    double t_min = INFINITY;
+    for (int rep = 0; rep < 3; ++rep) {  // the first run builds graphs and warms caches
+      pmcmc_info info{};
+      CK(cudaEventRecord(sc.ev[0], h->stream));
+      rc = solve_blocks(h, tg, p, b, seed, 0, T, b + bx, b + bx + bS, b + bx + bS + blp,
+                        PMCMC_MEM_DEVICE, &info);
+      if (rc) return rc;
+      CK(cudaEventRecord(sc.ev[1], h->stream));
+      CK(cudaEventSynchronize(sc.ev[1]));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, sc.ev[0], sc.ev[1]));
+      if (rep > 0) t_min = std::min(t_min, static_cast<double>(ms));
+    }
+    if (t_min < best_t) {
+      best_t = t_min;
+      best = c;
+    }
+  }
+  tune_put(key, best);
+  if (choice) *choice = best;
+  if (best_ms) *best_ms = best_t;
+  return PMCMC_OK;
+}
+
 int pmcmc_deer_solve(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
                      const void* x0, uint64_t seed, uint64_t block, void* S_out, void* logp_out,
                      uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
@@ -2139,7 +2272,7 @@ int pmcmc_slice_local(pmcmc_handle* h, const void* xbar0, void* agg, int32_t mem
   CK(cudaMemcpyAsync(h->d_params, &sl.P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
   const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
-  if (smem > 48 * 1024)
+  if (smem > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(k.eval), smem));
   const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
                                                       int64_t(h->num_sms) * 8));
@@ -2224,7 +2357,7 @@ int pmcmc_slice_result(pmcmc_handle* h, const void* xbar0, void* S_out, void* lo
                      h->stream));
   const SweepKernels k = gauss_sweep_kernels(es == 8, sl.tg->kind, sl.p.jacobian, D);
   const size_t smem = gauss_sweep_smem(es == 8, Dp, 1, sl.tg->kind == kDenseGauss).total;
-  if (smem > 48 * 1024)
+  if (smem > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(k.finalize), smem));
   const int grid = static_cast<int>(std::min<int64_t>((W + kWarps - 1) / kWarps,
                                                       int64_t(h->num_sms) * 8));

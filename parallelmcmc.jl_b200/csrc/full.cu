@@ -971,7 +971,7 @@ cudaError_t full_adjoint(cudaStream_t s, const DevParams* Pg, const FullArgs* Fg
   const size_t st = eval_smem_bytes(Dp, dense);
   const void* tk = dense ? reinterpret_cast<const void*>(&adjoint_terms_kernel<kDenseGauss>)
                          : reinterpret_cast<const void*>(&adjoint_terms_kernel<kDiagGauss>);
-  if (st > 48 * 1024) {
+  if (st > 0) {
     e = raise_smem_limit(reinterpret_cast<const void*>(tk), st);
     if (e != cudaSuccess) return e;
   }
@@ -1010,7 +1010,7 @@ cudaError_t full_adjoint(cudaStream_t s, const DevParams* Pg, const FullArgs* Fg
                     sizeof(float) * ((dense ? Dp * Dp : 0) + kWarps * Dp);
   const void* rk = dense ? reinterpret_cast<const void*>(&adjoint_reduce_kernel<kDenseGauss>)
                          : reinterpret_cast<const void*>(&adjoint_reduce_kernel<kDiagGauss>);
-  if (sr > 48 * 1024) {
+  if (sr > 0) {
     e = raise_smem_limit(reinterpret_cast<const void*>(rk), sr);
     if (e != cudaSuccess) return e;
   }

@@ -123,7 +123,9 @@ __global__ void __launch_bounds__(kThreads)
 cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
   static std::mutex mu;
   static std::unordered_map<const void*, size_t> limit;
-  if (bytes <= 48 * 1024) return cudaSuccess;
+  // (also below 48 KB: static plus dynamic shared memory above 48 KB needs the
+  // opt-in even when the dynamic part alone is under it)
+  if (bytes == 0) return cudaSuccess;
   std::lock_guard<std::mutex> lk(mu);
   size_t& cur = limit[fn];
   if (bytes <= cur) return cudaSuccess;
@@ -160,13 +162,13 @@ cudaError_t launch_affine_scan(cudaStream_t s, bool f64, int64_t D, int64_t T, c
   cudaError_t e = cudaMemsetAsync(scr.counter, 0, 2 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   if (f64) {
-    if (smem > 48 * 1024)
+    if (smem > 0)
       raise_smem_limit(reinterpret_cast<const void*>(affine_scan_kernel<double>), smem);
     affine_scan_kernel<double><<<ntiles, kThreads, smem, s>>>(
         D, T, TT, static_cast<const double*>(A), static_cast<const double*>(B),
         static_cast<const double*>(s0), static_cast<double*>(S), scr, epoch);
   } else {
-    if (smem > 48 * 1024)
+    if (smem > 0)
       raise_smem_limit(reinterpret_cast<const void*>(affine_scan_kernel<float>), smem);
     affine_scan_kernel<float><<<ntiles, kThreads, smem, s>>>(
         D, T, TT, static_cast<const float*>(A), static_cast<const float*>(B),

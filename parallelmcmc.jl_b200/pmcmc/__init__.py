@@ -9,7 +9,8 @@ from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupp
                    default_handle, load)
 from .adapt import AdaptiveMALASampler, adapt_step_size, dual_average_update
 from .core import (Chain, DensityModel, ParallelMALASampler, ParallelMALAState,
-                   ParallelMALATransition, adjoint, fleet_solve, mala_chains, sample, solve,
+                   ParallelMALATransition, adjoint, autotune, fleet_solve, mala_chains, sample,
+                   solve,
                    solve_affine_scan_diag, step, tape)
 
 # Module-style aliases matching ParallelMCMC.DEER / ParallelMCMC.DEERScan.
@@ -20,6 +21,6 @@ __all__ = [
     "ArgumentError", "DimensionMismatch", "DeviceError", "Unsupported", "Handle",
     "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
     "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
-    "step", "tape", "mala_chains", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
+    "step", "tape", "mala_chains", "autotune", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
     "solve_affine_scan_diag", "DEER", "DEERScan",
 ]

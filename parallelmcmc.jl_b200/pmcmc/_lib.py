@@ -27,7 +27,7 @@ SYMBOLS = [
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
     "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
-    "pmcmc_fleet_solve", "pmcmc_check_wait_bound", "pmcmc_mala_chains",
+    "pmcmc_fleet_solve", "pmcmc_check_wait_bound", "pmcmc_mala_chains", "pmcmc_autotune",
 ]
 OBJECTIVE = {"esjd": 0, "mean_sq": 1}
 WAIT_KIND = {"lookback": 0, "mbarrier": 1}
@@ -138,6 +138,8 @@ def load(path: str = LIB_PATH):
         L.pmcmc_deer_adjoint.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64,
                                          C.c_uint64, _vp, C.c_int32, C.c_int32, _vp]
         L.pmcmc_check_wait_bound.argtypes = [_vp, C.c_int32, C.POINTER(C.c_double)]
+        L.pmcmc_autotune.argtypes = [_vp, _vp, C.POINTER(DeerParams), _vp, C.c_uint64, C.c_int32,
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         L.pmcmc_mala_chains.argtypes = [_vp, _vp, C.POINTER(DeerParams), C.c_int64, _vp, _vp,
                                         C.c_uint64, _vp, _vp, _vp, C.c_int32]
         for fn in SYMBOLS:

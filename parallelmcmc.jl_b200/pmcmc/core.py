@@ -385,6 +385,24 @@ def solve(model: DensityModel, sampler: ParallelMALASampler, s0, *, seed: int = 
     return Sv, info.as_dict()
 
 
+# --------------------------------------------------------------------------- autotuning
+def autotune(model: DensityModel, sampler: ParallelMALASampler, x0, *, seed: int = 0,
+             handle: Optional[L.Handle] = None, device: int = 0) -> dict:
+    """Time the candidate kernel shapes for this problem on the device and keep
+    the fastest for later solves of the same shape (pmcmc_autotune).  Returns
+    {"choice": kept value (CTAs a SM, or :full chunk count; 0 if nothing to
+    tune), "ms": its time a solve}."""
+    h = handle or L.default_handle(device)
+    tgt = model.device_target(h)
+    keep, x0p, mem = _input_vector(x0, model.dim, sampler.dtype, None)
+    ch = C.c_int32(0)
+    ms = C.c_double(0.0)
+    p = sampler.params()
+    L.check(L.load().pmcmc_autotune(h.ptr, tgt, C.byref(p), x0p, int(seed), mem, C.byref(ch),
+                                    C.byref(ms)), h.ptr, "autotune")
+    return {"choice": int(ch.value), "ms": float(ms.value)}
+
+
 # --------------------------------------------------------------------------- sequential chains
 def mala_chains(model: DensityModel, sampler: ParallelMALASampler, x0s, seeds, *,
                 block: int = 0, handle: Optional[L.Handle] = None, device: int = 0):
