@@ -16,6 +16,12 @@
 // hi*hi + hi*lo + lo*hi with FP32 accumulation.  Tangent columns (only used
 // for the Jacobian estimate) and s use a single FP16 term.
 //
+// The MMAs are bound by shared-memory reads of the X operand at these widths,
+// so each k step issues two: Xh [Bh | Bt | Bl] (N = 96, the hi*lo product in
+// accumulator columns of its own, added in the epilogue) and Xl Bh (N = 32,
+// accumulated onto the hi*hi columns).  GEMM2 is arranged the same way with
+// [Rh | S | Rl].
+//
 // Roles: warps 0-15 run the epilogue (warps w, w+4, w+8, w+12 share TMEM lane
 // quarter w % 4 and take 8 columns each); lane 0 of warp 16 issues TMA loads
 // and MMAs and warp 16 owns the TMEM allocation.
@@ -41,15 +47,17 @@ constexpr int kThreadsTC = 544;  // 16 epilogue warps + 1 producer warp
 constexpr int kEpi = 16;
 constexpr int kProd = 16;  // producer / TMEM-owner warp
 constexpr int kParts = kEpi / 4;  // epilogue warps per TMEM lane quarter
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // L at 0, G half h at 128 (h + 1); 96 columns each
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at B200 clocks
 constexpr uint32_t kBoxX = BN * 128;       // one 64-wide d box of X: 128 rows x 128 B
-constexpr uint32_t kBoxB1 = 2 * BT * 128;  // value hi rows | tangent rows
-constexpr uint32_t kBoxBl = BT * 128;      // value lo rows
-constexpr uint32_t kRBlock = (BN / 8) * 128;  // one 8-column block of R: 16 core matrices
+constexpr uint32_t kBoxB = 3 * BT * 128;  // value hi rows | tangent rows | value lo rows
+// R (GEMM2's B operand, N = 96 columns [r hi | s | r lo] by K = BN rows) is
+// MN-major with the 128-byte swizzle, like X^T: two 64-column atoms of BN rows
+// x 128 B; chunk c (8 columns) of row k sits at chunk c ^ (k & 7).
+constexpr uint32_t kRAtom = BN * 128;
 
 struct Layout {
-  uint32_t xh, xl, b1, bl, r, bars, total;
+  uint32_t xh, xl, b, r, bars, total;
 };
 
 __host__ __device__ inline Layout layout(int nkb) {
@@ -59,12 +67,10 @@ __host__ __device__ inline Layout layout(int nkb) {
   off += nkb * kBoxX;
   L.xl = off;
   off += nkb * kBoxX;
-  L.b1 = off;
-  off += nkb * kBoxB1;
-  L.bl = off;
-  off += nkb * kBoxBl;
+  L.b = off;
+  off += nkb * kBoxB;
   L.r = off;
-  off += 12 * kRBlock;
+  off += 2 * kRAtom;
   L.bars = off;
   off += 128;
   L.total = off + 1024;  // slack for 1024-B alignment of the dynamic window
@@ -170,34 +176,29 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 16 consecutive FP32 TMEM columns of this warp's 32 lanes.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
+// Three 8-column TMEM loads of this warp's 32 lanes, then one wait.  The wait
+// is in the same asm statement as the loads, so no use of the registers can
+// move above it.
+__device__ __forceinline__ void tmem_ld8x3(uint32_t ta, uint32_t tb, uint32_t tc, float (&a)[8],
+                                           float (&b)[8], float (&c)[8]) {
+  uint32_t r[24];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%24];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8, %9, %10, %11, %12, %13, %14, %15}, [%25];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16, %17, %18, %19, %20, %21, %22, %23}, [%26];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr)
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23])
+      : "r"(ta), "r"(tb), "r"(tc)
       : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 8 consecutive FP32 TMEM columns of this warp's 32 lanes.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-  uint32_t r[8];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7])
-      : "r"(taddr)
-      : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 8; ++i) {
+    a[i] = __uint_as_float(r[i]);
+    b[i] = __uint_as_float(r[8 + i]);
+    c[i] = __uint_as_float(r[16 + i]);
+  }
 }
 
 // Shared-memory matrix descriptor (tcgen05): start, leading / stride byte
@@ -219,18 +220,35 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn, bool b
          (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-template <int NH>
-__device__ __forceinline__ uint4 pack8(const __half (&h)[NH], int b) {
-  uint4 u;
-  u.x = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 0])) |
-        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 1])) << 16);
-  u.y = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 2])) |
-        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 3])) << 16);
-  u.z = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 4])) |
-        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 5])) << 16);
-  u.w = static_cast<uint32_t>(__half_as_ushort(h[8 * b + 6])) |
-        (static_cast<uint32_t>(__half_as_ushort(h[8 * b + 7])) << 16);
-  return u;
+// log(1 + e) for e in [0, 1]: e q(e), q the degree-9 Chebyshev least-squares
+// fit of log1p(e) / e on [0, 1] written in powers of e with FP32 coefficients.
+// Absolute error below 1.3e-7 on [0, 1] (a correctly rounded FP32 log1p has
+// 6e-8; the FP32 rounding of the log-likelihood term it enters is larger than
+// either).  FMAs only: no division, no special-function unit.
+__device__ __forceinline__ float log1p_unit(float e) {
+  float q = -0.0032140363473445177f;
+  q = fmaf(q, e, 0.019649166613817215f);
+  q = fmaf(q, e, -0.056435029953718185f);
+  q = fmaf(q, e, 0.10533228516578674f);
+  q = fmaf(q, e, -0.1525145173072815f);
+  q = fmaf(q, e, 0.19651491940021515f);
+  q = fmaf(q, e, -0.24947808682918549f);
+  q = fmaf(q, e, 0.3332909941673279f);
+  q = fmaf(q, e, -0.4999985098838806f);
+  q = fmaf(q, e, 1.0f);
+  return e * q;
+}
+
+// Two FP32 values as one FP16x2 word (a in the low half), one conversion.
+__device__ __forceinline__ uint32_t half2_bits(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// hi = x with its low 13 mantissa bits cleared: exact in FP16 for
+// 2^-14 <= |x| < 65504, and x - hi is exact in FP32 (|x - hi| < 2^-10 |x|).
+__device__ __forceinline__ float split_hi(float x) {
+  return __uint_as_float(__float_as_uint(x) & 0xffffe000u);
 }
 
 // G (Dp x 2T column-major: value block then tangent block, FP32) and lp (T,
@@ -251,19 +269,18 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   const Layout Ly = layout(nkb);
   unsigned char* sXh = base + Ly.xh;
   unsigned char* sXl = base + Ly.xl;
-  unsigned char* sB1 = base + Ly.b1;
-  unsigned char* sBl = base + Ly.bl;
+  unsigned char* sB = base + Ly.b;
   unsigned char* sR = base + Ly.r;
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + Ly.bars);
-  // X moves in K halves h (boxes kb in [h nkb/nh, (h+1) nkb/nh)): GEMM2's
-  // d-half h reads exactly X's K half h, so the next block's half h loads
-  // while GEMM2's later half and GEMM1's earlier half run.
+  // X moves box by box (64 values of d, hi and lo): GEMM2's d-half h reads
+  // exactly boxes 2h and 2h + 1, so the next block's boxes of half h load
+  // while GEMM2's later half runs, and GEMM1 starts on box 0 as soon as it lands.
   uint64_t* bar_b = bars + 0;  // B tile loaded
-  uint64_t* bar_x = bars + 1;  // [2] X K half h loaded
-  uint64_t* bar_l = bars + 3;  // GEMM1 done (L ready)
-  uint64_t* bar_r = bars + 4;  // epilogue wrote R (256 arrivals)
-  uint64_t* bar_g = bars + 5;  // [2] GEMM2 half h done (X K half h free; R free after the last)
-  uint64_t* bar_z = bars + 7;  // teardown drain
+  uint64_t* bar_x = bars + 1;  // [4] X box kb loaded
+  uint64_t* bar_l = bars + 5;  // GEMM1 done (L ready)
+  uint64_t* bar_r = bars + 6;  // epilogue wrote R (32 kEpi arrivals)
+  uint64_t* bar_g = bars + 7;  // [2] GEMM2 half h done (X boxes of half h free; R free after the last)
+  uint64_t* bar_z = bars + 9;  // teardown drain
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   __shared__ double s_red[kEpi][BT / kParts];
@@ -276,8 +293,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 
   if (threadIdx.x == 0) {
     mbar_init(bar_b, 1);
-    mbar_init(bar_x, 1);
-    mbar_init(bar_x + 1, 1);
+    for (int kb = 0; kb < 4; ++kb) mbar_init(bar_x + kb, 1);
     mbar_init(bar_l, 1);
     mbar_init(bar_r, 32 * kEpi);
     mbar_init(bar_g, 1);
@@ -291,67 +307,64 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t tL = tmem;         // columns [0, 64): value | tangent logits
-  const uint32_t tG = tmem + 64;    // half h at [64 + 64h, 128 + 64h)
+  // L: columns [0, 96) = value (hi*hi + lo*hi) | tangent | value hi*lo.
+  // G half h: columns [128 (h + 1), 128 (h + 1) + 96), the same three parts.
+  const uint32_t tL = tmem;
+  const uint32_t tG = tmem + 128;
 
   if (warp == kProd) {
     if (lane == 0) {
       bool ok = true;
-      const uint32_t i1_vt = idesc_f16(128, has_tangent ? 2 * BT : BT, false, false);
+      const uint32_t i1_all = idesc_f16(128, 3 * BT, false, false);
       const uint32_t i1_v = idesc_f16(128, BT, false, false);
-      const uint32_t i2_rs = idesc_f16(128, has_tangent ? 2 * BT : BT, true, true);
-      const uint32_t i2_r = idesc_f16(128, BT, true, true);
-      mbar_expect_tx(bar_b, nkb * (has_tangent ? kBoxB1 : kBoxB1 / 2) + nkb * kBoxBl);
+      const uint32_t i2_all = idesc_f16(128, 3 * BT, true, true);
+      const uint32_t i2_v = idesc_f16(128, BT, true, true);
+      mbar_expect_tx(bar_b, nkb * kBoxB);
       for (int kb = 0; kb < nkb; ++kb) {
-        tma_2d(sB1 + kb * kBoxB1, &tmBh, kb * 64, static_cast<int>(t0), bar_b);
-        if (has_tangent) tma_2d(sB1 + kb * kBoxB1 + BT * 128, &tmBt, kb * 64, static_cast<int>(t0), bar_b);
-        tma_2d(sBl + kb * kBoxBl, &tmBl, kb * 64, static_cast<int>(t0), bar_b);
+        unsigned char* b = sB + kb * kBoxB;
+        tma_2d(b, &tmBh, kb * 64, static_cast<int>(t0), bar_b);
+        // without tangent columns the middle rows repeat Bh: the MMA reads
+        // them and nothing uses their products
+        tma_2d(b + BT * 128, has_tangent ? &tmBt : &tmBh, kb * 64, static_cast<int>(t0), bar_b);
+        tma_2d(b + 2 * BT * 128, &tmBl, kb * 64, static_cast<int>(t0), bar_b);
       }
       ok = mbar_wait(bar_b, 0, err);
-      const int kbh = nkb / nh;  // X boxes per K half
-      auto load_x = [&](int nb, int h) {
-        mbar_expect_tx(bar_x + h, 2 * kbh * kBoxX);
-        for (int kb = h * kbh; kb < (h + 1) * kbh; ++kb) {
-          tma_2d(sXh + kb * kBoxX, &tmXh, kb * 64, nb * BN, bar_x + h);
-          tma_2d(sXl + kb * kBoxX, &tmXl, kb * 64, nb * BN, bar_x + h);
-        }
+      auto load_x = [&](int nb, int kb) {
+        mbar_expect_tx(bar_x + kb, 2 * kBoxX);
+        tma_2d(sXh + kb * kBoxX, &tmXh, kb * 64, nb * BN, bar_x + kb);
+        tma_2d(sXl + kb * kBoxX, &tmXl, kb * 64, nb * BN, bar_x + kb);
       };
       if (ok)
-        for (int h = 0; h < nh; ++h) load_x(0, h);
+        for (int kb = 0; kb < nkb; ++kb) load_x(0, kb);
       for (int nb = 0; nb < nblocks && ok; ++nb) {
-        // GEMM1: L = Xh [Bh | Bt] + Xh Bl + Xl Bh, K half by K half as X arrives
-        for (int h = 0; h < nh; ++h) {
-          if (!(ok = mbar_wait(bar_x + h, nb & 1, err))) break;
+        // GEMM1: L = Xh [Bh | Bt | Bl] + Xl Bh, box by box as X arrives
+        for (int kb = 0; kb < nkb; ++kb) {
+          if (!(ok = mbar_wait(bar_x + kb, nb & 1, err))) break;
           tc_fence_after();
-          for (int kb = h * kbh; kb < (h + 1) * kbh; ++kb)
 #pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-              const uint64_t ah = sdesc(su32(sXh + kb * kBoxX) + ks * 32, 16, 1024, 2);
-              const uint64_t al = sdesc(su32(sXl + kb * kBoxX) + ks * 32, 16, 1024, 2);
-              const uint64_t bhz = sdesc(su32(sB1 + kb * kBoxB1) + ks * 32, 16, 1024, 2);
-              const uint64_t bl = sdesc(su32(sBl + kb * kBoxBl) + ks * 32, 16, 1024, 2);
-              mma_f16(tL, ah, bhz, i1_vt, (kb | ks) != 0);
-              mma_f16(tL, ah, bl, i1_v, 1);
-              mma_f16(tL, al, bhz, i1_v, 1);
-            }
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint64_t ah = sdesc(su32(sXh + kb * kBoxX) + ks * 32, 16, 1024, 2);
+            const uint64_t al = sdesc(su32(sXl + kb * kBoxX) + ks * 32, 16, 1024, 2);
+            const uint64_t bb = sdesc(su32(sB + kb * kBoxB) + ks * 32, 16, 1024, 2);
+            mma_f16(tL, ah, bb, i1_all, (kb | ks) != 0);
+            mma_f16(tL, al, bb, i1_v, 1);
+          }
         }
         if (!ok) break;
         mma_commit(bar_l);
         if (!(ok = mbar_wait(bar_r, nb & 1, err))) break;
         tc_fence_after();
-        // GEMM2: G_h += Xh^T [Rh | S] + Xh^T Rl + Xl^T Rh  (A MN-major, B MN-major)
+        // GEMM2: G_h += Xh^T [Rh | S | Rl] + Xl^T Rh  (A MN-major, B MN-major)
         for (int h = 0; h < nh; ++h) {
           if (has_g) {
 #pragma unroll
             for (int kn = 0; kn < BN / 16; ++kn) {
               const uint64_t ah = sdesc(su32(sXh + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
               const uint64_t al = sdesc(su32(sXl + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
-              const uint64_t brs = sdesc(su32(sR) + kn * 256, 128, kRBlock, 0);
-              const uint64_t brl = sdesc(su32(sR + 8 * kRBlock) + kn * 256, 128, kRBlock, 0);
+              const uint64_t br = sdesc(su32(sR) + kn * 2048, kRAtom, 1024, 2);
               const uint32_t acc = (nb > 0 || kn > 0) ? 1u : 0u;
-              mma_f16(tG + 64 * h, ah, brs, i2_rs, acc);
-              mma_f16(tG + 64 * h, ah, brl, i2_r, 1);
-              mma_f16(tG + 64 * h, al, brs, i2_r, 1);
+              mma_f16(tG + 128 * h, ah, br, i2_all, acc);
+              mma_f16(tG + 128 * h, al, br, i2_v, 1);
             }
           }
           mma_commit(bar_g + h);
@@ -360,7 +373,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         if (nb + 1 < nblocks)
           for (int h = 0; h < nh; ++h) {
             if (!(ok = mbar_wait(bar_g + h, nb & 1, err))) break;
-            load_x(nb + 1, h);
+            load_x(nb + 1, 2 * h);
+            load_x(nb + 1, 2 * h + 1);
           }
       }
       if (!ok) {
@@ -379,9 +393,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     const uint32_t lane_off = static_cast<uint32_t>(quarter * 32) << 16;
     constexpr int BH = BT / kParts;
     static_assert(BH == 8, "one 8-column block of R a thread");
-    double lacc[BH];
+    // log-likelihood sums, compensated (Kahan) in FP32: ls the sum, lc the
+    // running error; the column total is ls - lc, formed in FP64 at the end
+    float ls[BH], lc[BH];
 #pragma unroll
-    for (int t = 0; t < BH; ++t) lacc[t] = 0.0;
+    for (int t = 0; t < BH; ++t) ls[t] = lc[t] = 0.f;
     bool ok = true;
     float y_next = row < N ? __ldg(ylab + row) : 0.f;  // label of this row, one block ahead
     for (int nb = 0; nb < nblocks; ++nb) {
@@ -391,28 +407,41 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
-      float v[BH], w[BH];
-      tmem_ld8(tL + lane_off + BH * part, v);
-      if (has_tangent) tmem_ld8(tL + lane_off + BT + BH * part, w);
-      __half rh[BH], rl[BH], sh[BH];
+      float v[BH], vl[BH], w[BH];
+      tmem_ld8x3(tL + lane_off + BH * part, tL + lane_off + 2 * BT + BH * part,
+                 tL + lane_off + BT + BH * part, v, vl, w);
+      float r[BH], s[BH];
 #pragma unroll
       for (int t = 0; t < BH; ++t) {
-        const float l = v[t];
+        const float l = v[t] + vl[t];
         const float e = __expf(-fabsf(l));
         const float inv = __fdividef(1.f, 1.f + e);
         const float p = l >= 0.f ? inv : e * inv;
-        const float r = valid ? yn - p : 0.f;
-        const float s = (valid && has_tangent) ? p * (1.f - p) * w[t] : 0.f;
-        if (valid) lacc[t] += static_cast<double>(yn * l - (fmaxf(l, 0.f) + log1pf(e)));
-        rh[t] = __float2half_rn(r);
-        rl[t] = __float2half_rn(r - __half2float(rh[t]));
-        sh[t] = __float2half_rn(s);
+        r[t] = valid ? yn - p : 0.f;
+        s[t] = (valid && has_tangent) ? p * (1.f - p) * w[t] : 0.f;
+        if (valid) {
+          const float y = (yn * l - (fmaxf(l, 0.f) + log1p_unit(e))) - lc[t];
+          const float sum = ls[t] + y;
+          lc[t] = (sum - ls[t]) - y;
+          ls[t] = sum;
+        }
       }
       if (has_g) {
-        const uint32_t roff = static_cast<uint32_t>((row >> 3) * 128 + (row & 7) * 16);
-        *reinterpret_cast<uint4*>(sR + (0 + part) * kRBlock + roff) = pack8(rh, 0);
-        *reinterpret_cast<uint4*>(sR + (4 + part) * kRBlock + roff) = pack8(sh, 0);
-        *reinterpret_cast<uint4*>(sR + (8 + part) * kRBlock + roff) = pack8(rl, 0);
+        // R columns as FP16: r split hi + lo, s one term; two values a conversion
+        uint32_t wh[BH / 2], wl[BH / 2], ws[BH / 2];
+#pragma unroll
+        for (int q = 0; q < BH / 2; ++q) {
+          const float h0 = split_hi(r[2 * q]), h1 = split_hi(r[2 * q + 1]);
+          wh[q] = half2_bits(h0, h1);
+          wl[q] = half2_bits(r[2 * q] - h0, r[2 * q + 1] - h1);
+          ws[q] = half2_bits(s[2 * q], s[2 * q + 1]);
+        }
+        // value hi: atom 0 chunk part; s: atom 0 chunk 4 + part; value lo: atom 1 chunk part
+        unsigned char* rrow = sR + row * 128;
+        const int sw = row & 7;
+        *reinterpret_cast<uint4*>(rrow + ((part ^ sw) << 4)) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+        *reinterpret_cast<uint4*>(rrow + (((4 + part) ^ sw) << 4)) = make_uint4(ws[0], ws[1], ws[2], ws[3]);
+        *reinterpret_cast<uint4*>(rrow + kRAtom + ((part ^ sw) << 4)) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
         fence_async_smem();
       }
       tc_fence_before();
@@ -424,7 +453,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (part < 2 * nh) {
         const int h = part >> 1, b = part & 1;
         float g[32];
-        tmem_ld32(tG + 64 * h + lane_off + BT * b, g);
+        tmem_ld32(tG + 128 * h + lane_off + BT * b, g);
+        if (b == 0) {  // value columns: add the hi*lo part
+          float gl[32];
+          tmem_ld32(tG + 128 * h + lane_off + 2 * BT, gl);
+#pragma unroll
+          for (int t = 0; t < BT; ++t) g[t] += gl[t];
+        }
         const int64_t d = 128 * h + row;
         if (d < Dp) {
           const int64_t cbase = b ? T : 0;
@@ -438,7 +473,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     }
 #pragma unroll
     for (int t = 0; t < BH; ++t) {
-      const double sum = warp_sum(lacc[t]);
+      const double sum = warp_sum(static_cast<double>(ls[t]) - static_cast<double>(lc[t]));
       if (lane == 0) s_red[warp][t] = sum;
     }
     asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpi) : "memory");
