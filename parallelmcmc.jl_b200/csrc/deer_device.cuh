@@ -192,43 +192,39 @@ __device__ void tile_scan_inplace(Real* As, Real* Bs, int ncols, int D, int Dp) 
   }
 }
 
-// Decoupled look-back (Merrill & Garland), windowed: warp 0 polls the flags of
-// the 32 nearest predecessors at once and returns the nearest tile j* whose
-// inclusive state is published; every tile in (j*, tile) has published at
-// least its aggregate.  Waits are bounded: on timeout *err = 1 and -1 is
+// Decoupled look-back (Merrill & Garland) with a fixed association: `tile`
+// composes the aggregates of the tiles (jd, tile) onto the inclusive state of
+// jd, the last tile of the previous group of 32 (tile 0 for the first group).  The composition, and so
+// the FP rounding, is the same in every run, whichever tile finished first.
+// Lane l of warp 0 waits for tile jd + l (its inclusive state for l = 0, its
+// aggregate otherwise).  Waits are bounded: on timeout *err = 1 and -1 is
 // returned (the caller records the error and carries on, never hangs).
-__device__ __forceinline__ int lookback_window(int tile, uint32_t epoch, const uint32_t* flags,
-                                               int* err) {
+constexpr int kLookGroup = 32;
+__device__ __forceinline__ int lookback_fixed(int tile, uint32_t epoch, const uint32_t* flags,
+                                              int* err) {
   const int lane = threadIdx.x & 31;
   const uint32_t ep = epoch & 0x3fffffffu;
-  for (int hi = tile - 1; hi >= 0; hi -= 32) {
-    const int j = hi - lane;
-    uint32_t st = 0;
-    bool timeout = false;
-    if (j >= 0) {
-      long long spins = 0;
-      while (true) {
-        const uint32_t f = ld_acquire(flags + j);
-        if ((f >> 2) == ep && (f & 3u)) {
-          st = f & 3u;
-          break;
-        }
-        if (++spins > kMaxSpins) {
-          timeout = true;
-          break;
-        }
-        if (spins > 16) __nanosleep(32);
+  const int jd = tile < kLookGroup ? 0 : (tile / kLookGroup) * kLookGroup - 1;
+  const int j = jd + lane;
+  bool timeout = false;
+  if (j < tile) {
+    const uint32_t need = lane == 0 ? kFlagIncl : kFlagAgg;
+    long long spins = 0;
+    while (true) {
+      const uint32_t f = ld_acquire(flags + j);
+      if ((f >> 2) == ep && (f & 3u) >= need) break;
+      if (++spins > kMaxSpins) {
+        timeout = true;
+        break;
       }
+      if (spins > 16) __nanosleep(32);
     }
-    if (__any_sync(0xffffffffu, timeout)) {
-      *err = 1;
-      return -1;
-    }
-    const unsigned incl = __ballot_sync(0xffffffffu, j >= 0 && st == kFlagIncl);
-    if (incl) return hi - (__ffs(incl) - 1);
   }
-  *err = 1;  // tile 0 always publishes an inclusive state, so this is unreachable
-  return -1;
+  if (__any_sync(0xffffffffu, timeout)) {
+    *err = 1;
+    return -1;
+  }
+  return jd;
 }
 
 // State entering `tile` for coordinate d: the aggregates of tiles (jstar, tile)

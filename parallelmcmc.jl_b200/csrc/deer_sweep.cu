@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kThreads)
         if (tid == 0) st_release(P.flags + tile, (epoch << 2) | kFlagAgg);
         if (warp == 0) {
           int err = 0;
-          const int js = lookback_window(tile, epoch, P.flags, &err);
+          const int js = lookback_fixed(tile, epoch, P.flags, &err);
           if (lane == 0) {
             s_jstar = js;
             if (err) s_err = 1;

@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kThreads)
     if (tid == 0) st_release(scr.flags + tile, (epoch << 2) | kFlagAgg);
     if ((tid >> 5) == 0) {
       int err = 0;
-      const int js = lookback_window(tile, epoch, scr.flags, &err);
+      const int js = lookback_fixed(tile, epoch, scr.flags, &err);
       if (tid == 0) {
         s_jstar = js;
         if (err) s_err = 1;
@@ -313,11 +313,11 @@ cudaError_t launch_broadcast(cudaStream_t s, bool f64, int64_t Dp, int64_t T, co
 
 // Bound check of the look-back wait: one warp looks back from tile 1 over a
 // flag array that nothing publishes (all zeros: no epoch, no state), so lane 0
-// spins until kMaxSpins and the warp reports the give-up in err[0].  The same
+// spins on tile 0 until kMaxSpins and the warp reports the give-up in err[0].  The same
 // routine guards every scan and sweep launch.
 __global__ void lookback_bound_kernel(const uint32_t* flags, int* err) {
   int e = 0;
-  lookback_window(1, 1u, flags, &e);
+  lookback_fixed(1, 1u, flags, &e);
   if (threadIdx.x == 0) err[0] = e;
 }
 
