@@ -39,6 +39,7 @@ sys.path.insert(0, os.path.join(ROOT, "parallelmcmc.jl_b200"))
 METRIC = "DEER samples/sec, batched+mixed vs plain GPU DEER, at trace err ≤1e-5 vs FP64"
 WORKLOAD = "diag_gauss_D100_T16384_diag_f32"
 E2E_BLOCKS = 8  # blocks of T samples per end-to-end sample() call
+STEP_BLOCKS = 8  # blocks of T samples per timed device-resident sample() call
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 L2_FLUSH_BYTES = 512 << 20
 
@@ -237,24 +238,53 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         return [a.elapsed_time(b) for a, b in ev], infos
 
+    # A step is one sample() call of STEP_BLOCKS blocks into HBM buffers: block b + 1
+    # starts from block b's last column on the device, the blocks run back to back.
+    S_run = torch.empty((STEP_BLOCKS * T, D), dtype=torch.float32, device=dev)
+    lp_run = torch.empty((STEP_BLOCKS * T,), dtype=torch.float32, device=dev)
+    acc_run = torch.empty((STEP_BLOCKS * T,), dtype=torch.uint8, device=dev)
+
+    def timed_run(smp, nsteps, seed0):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(nsteps)]
+        infos = []
+        for k in range(nsteps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            info = L.Info()
+            p = smp.params()
+            rc = lib.pmcmc_sample(h.ptr, tgt, C.byref(p), x0_dev.data_ptr(), seed0 + k,
+                                  STEP_BLOCKS * T, S_run.data_ptr(), lp_run.data_ptr(),
+                                  acc_run.data_ptr(), L.MEM_DEVICE, C.byref(info))
+            L.check(rc, h.ptr, "sample")
+            ev[k][1].record(stream)
+            infos.append(info)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in ev], infos
+
     # ---- warm-up and timed region (device-resident inputs/outputs)
-    timed(sampler, args.warmup, 0)
+    timed_run(sampler, args.warmup, seed + 100)
     if pg:
         pg.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        ms, infos = timed(sampler, args.steps, 1000)
+        ms, infos = timed_run(sampler, args.steps, seed + 1000)
     torch.cuda.synchronize(dev)
     total_ms = sum(ms)
     if pg:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * args.steps * T / (total_ms / 1e3)
-    iters = [i.iters for i in infos]
+    value = world * args.steps * STEP_BLOCKS * T / (total_ms / 1e3)
+    iters = [i.iters / STEP_BLOCKS for i in infos]  # Newton sweeps a block
     persistent = bool(infos[0].path & 32)
     # one cooperative launch per block (persistent solve), else init + sweeps + finalize
-    launches = sum(1 if persistent else 2 + i.iters for i in infos)
+    launches = sum(STEP_BLOCKS * (1 if persistent else 2) + (0 if persistent else i.iters)
+                   for i in infos)
+    # the same blocks one solve() call each (a host round trip between blocks)
+    timed(sampler, 2, 0)
+    ms1, _ = timed(sampler, args.steps, 1000)
+    value_one_call = world * args.steps * T / (sum(ms1) / 1e3)
 
     # ---- parity of the timed workload: first timed block vs the FP64 sequential oracle
     parity = {}
@@ -279,9 +309,9 @@ def run_ours(args):
     # ---- plain GPU DEER (unfused, reference-structured) on the same workload
     plain = pmcmc.ParallelMALASampler(sampler.epsilon, T=T, jacobian=sampler.jacobian,
                                       dtype=np.float32, exec="plain")
-    timed(plain, 1, 0)
-    pms, pinfos = timed(plain, max(3, args.steps // 4), 2000)
-    plain_value = len(pms) * T / (sum(pms) / 1e3)
+    timed_run(plain, 1, seed + 1900)
+    pms, pinfos = timed_run(plain, max(3, args.steps // 4), seed + 2000)
+    plain_value = len(pms) * STEP_BLOCKS * T / (sum(pms) / 1e3)
 
     # ---- roofline of the dominant kernel (the fused sweep), CUDA events per launch
     h.set_profiling(True)
@@ -381,6 +411,10 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded NumPy PCG64 + counter-based Philox tape)",
             "config": {"workload": WORKLOAD, "D": D, "T": T, "eps": 0.05, "jacobian": "diag",
+                       "step": f"pmcmc_sample of {STEP_BLOCKS} blocks (N={STEP_BLOCKS}*T) into "
+                               f"HBM buffers, x0 in HBM; CUDA events on the launching stream",
+                       "one_block_per_call": {"value": value_one_call, "unit": "samples/s",
+                                              "step": "pmcmc_deer_solve of one block"},
                        "state": "f32", "logalpha": "f64", "l2": "flushed (512 MB write) "
                        "between timed steps", "parallelism": f"replicas x{world}",
                        "newton_iters_mean": statistics.mean(iters),
@@ -397,7 +431,7 @@ def run_ours(args):
                                     "note": "independent taped MALA chains, one warp each "
                                             "(pmcmc_mala_chains), same block and tape"},
             "plain_gpu": {"value": plain_value, "unit": "samples/s",
-                          "newton_iters_mean": statistics.mean(i.iters for i in pinfos),
+                          "newton_iters_mean": statistics.mean(i.iters / STEP_BLOCKS for i in pinfos),
                           "speedup_fused_over_plain": value / world / plain_value},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": src,

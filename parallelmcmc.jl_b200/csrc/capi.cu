@@ -1180,12 +1180,15 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   const int64_t nblocks = (N + T - 1) / T;
   // Host outputs of several blocks: block b's copy-out overlaps block b + 1's solve.
   const bool pipe = mem == PMCMC_MEM_HOST && nblocks > 1;
+  // Several blocks: each block's state goes to a pinned ring, read after the last
+  // block, so the blocks run back to back with no host round trip between them.
+  const bool defer = nblocks > 1;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
                                use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr,
                                false, pipe);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
-  if (pipe) {
+  if (defer) {
     rc = ensure_pipeline(h, nblocks);
     if (rc) return rc;
   }
@@ -1289,7 +1292,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     P.ncols_out = nkeep;
     if (persist) {
       P.x0_src = (b == 0 && mem == PMCMC_MEM_DEVICE) ? x0 : P.x0;
-      P.st_host = pipe ? h->h_states + b : h->h_state;  // written by the kernel
+      P.st_host = defer ? h->h_states + b : h->h_state;  // written by the kernel
     }
     if (mem == PMCMC_MEM_DEVICE) {
       P.S_out = static_cast<unsigned char*>(S_out) + es * nsteps * D;
@@ -1328,7 +1331,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       if (pipe) CK(cudaEventRecord(h->ev_copy[slot], cs));
     }
     nsteps += nkeep;
-    if (pipe) {  // block states are read after the last block
+    if (defer) {  // block states are read after the last block
       if (!persist)
         CK(cudaMemcpyAsync(h->h_states + b, h->d_state, sizeof(DevState),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -1341,9 +1344,9 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     states[static_cast<size_t>(b)] = *h->h_state;
     if (h->h_state->status) break;
   }
-  if (pipe) {
+  if (defer) {
     CK(cudaStreamSynchronize(h->stream));
-    CK(cudaStreamSynchronize(h->copy_stream));
+    if (pipe) CK(cudaStreamSynchronize(h->copy_stream));
     for (int64_t b = 0; b < nblocks; ++b) {
       states[static_cast<size_t>(b)] = h->h_states[b];
       if (h->h_states[b].status) {  // the blocks after a failed one do not count

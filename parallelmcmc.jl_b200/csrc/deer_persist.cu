@@ -124,6 +124,15 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
   if (threadIdx.x == 0) P = Pv;  // parameters by value: no upload before the launch
   __syncthreads();
   cg::grid_group grid = cg::this_grid();
+  // totals of the verification pass, folded in by every CTA as it finishes,
+  // and the arrival counter (the grid barriers in between order these resets
+  // before every update)
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->fin_counter = 0;
+    st->n_accept = 0;
+    st->min_margin_bits = dbits(INFINITY);
+    st->max_defect_bits = 0;
+  }
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int CPW = 32 / LPC;                  // columns per warp
@@ -148,7 +157,6 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
   Real* Sb = static_cast<Real*>(P.S[0]);                   // last column of every CTA
 
   double* part = P.part;  // [c][4]: this sweep's max|dS|, max|S|, non-finite flag
-  double* part_fin = P.part + 4 * static_cast<size_t>(nctas);  // accepts, margin, defect
   Real* x0s = reinterpret_cast<Real*>(smem_raw + pp.x0);
   {  // start state, zero-padded to Dp
     const Real* src = static_cast<const Real*>(P.x0_src ? P.x0_src : P.x0);
@@ -455,35 +463,29 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       mm = min(mm, s_red[0][w]);
       md = max(md, s_red[2][w]);
     }
-    // accepted count (exact in a double), -margin (so that max is min), defect
-    part_fin[4 * cta] = static_cast<double>(a);
-    part_fin[4 * cta + 1] = -mm;
-    part_fin[4 * cta + 2] = md;
-  }
-  grid.sync();
-  if (cta != 0) return;
+    // accepted count, smallest margin and largest defect into the totals
+    // (margins and defects are non-negative: their bits order like the values,
+    // and a NaN defect sorts above every number); the last CTA to arrive writes
+    // the final state, the others leave without waiting at a grid barrier
+    atomicAdd(&st->n_accept, a);
+    atomicMin(&st->min_margin_bits, dbits(mm));
+    atomicMax(&st->max_defect_bits, dbits(md));
+    __threadfence();
+    const bool last = atomicAdd(&st->fin_counter, 1u) == static_cast<unsigned>(nctas - 1);
+    if (!last) return;
+    __threadfence();
 
-  // ---- CTA 0: totals of the verification pass and the final state ----
-  double nacc_tot = 0.0;
-  for (int i = tid; i < nctas; i += kThreads) nacc_tot += __ldcg(part_fin + 4 * i);
-  nacc_tot = warp_sum(nacc_tot);
-  __syncthreads();
-  if (lane == 0) s_red[1][warp] = nacc_tot;
-  __syncthreads();
-  double tot = 0.0;
-  for (int w = 0; w < kWarps; ++w) tot += s_red[1][w];
-  double neg_mm, maxdef, unused;
-  reduce_partials(part_fin, nctas, &s_red[0][0], unused, neg_mm, maxdef);
-  if (tid == 0) {
+    // ---- last CTA: the final state ----
+    const unsigned long long* tot = &st->n_accept;
     DevState f{};
     f.epoch = st->epoch;  // look-back epochs of the per-sweep path continue
     f.iter = iter;
     f.converged = converged;
     f.status = status;
     f.metric = metric;
-    f.n_accept = static_cast<unsigned long long>(tot);
-    f.min_margin_bits = dbits(-neg_mm);
-    f.max_defect_bits = dbits(maxdef);
+    f.n_accept = __ldcg(tot);
+    f.min_margin_bits = __ldcg(&st->min_margin_bits);
+    f.max_defect_bits = __ldcg(&st->max_defect_bits);
     *st = f;
     if (P.st_host) {
       *P.st_host = f;

@@ -371,6 +371,39 @@ def test_sample_host_pipeline_matches_device_output(h):
         assert a.info["iters"] == b.info["iters"] and a.info["converged"] == 1
 
 
+def test_sample_multiblock_per_sweep_paths_device_matches_host(h):
+    # multi-block calls read every block's state after the last block (no host
+    # round trip between blocks); the per-sweep paths (logistic, sliding window)
+    # copy each block's state into the pinned ring behind the block
+    torch = pytest.importorskip("torch")
+    X, y = _logistic_problem(400, 24, 35)
+    cases = [(pmcmc.DensityModel.logistic(X, y),
+              pmcmc.ParallelMALASampler(0.02, T=512, jacobian="stoch_diag", dtype=np.float32,
+                                        maxiter=80), 24),
+             (pmcmc.DensityModel.diag_gaussian(np.linspace(0.5, 4.0, 6)),
+              pmcmc.ParallelMALASampler(0.05, T=256, jacobian="diag", dtype=np.float32,
+                                        window=64), 6)]
+    for model, sampler, D in cases:
+        x0 = np.zeros(D, np.float32)
+        N = 3 * sampler.T + 17
+        a = pmcmc.sample(model, sampler, N, seed=9, initial_params=x0, handle=h)
+        b = pmcmc.sample(model, sampler, N, seed=9, initial_params=torch.from_numpy(x0).cuda(),
+                         handle=h)
+        np.testing.assert_array_equal(a.values, b.values.cpu().numpy())
+        np.testing.assert_array_equal(a.accepted, b.accepted.cpu().numpy())
+        assert a.info["iters"] == b.info["iters"] > 4
+        # block by block through solve(), chaining the last column, gives the same chain
+        xs, iters = x0.astype(np.float64), 0
+        for blk in range(4):
+            S, info, lp, acc = pmcmc.solve(model, sampler, xs.astype(np.float32), seed=9,
+                                           block=blk, handle=h, return_logp=True)
+            n = min(sampler.T, N - blk * sampler.T)
+            np.testing.assert_array_equal(S[:, :n].T, a.values[blk * sampler.T:blk * sampler.T + n])
+            xs = S[:, n - 1]
+            iters += info["iters"]
+        assert iters == a.info["iters"]
+
+
 def test_step_api_walks_and_resolves(h):
     # interface.jl:811-869, test-DEER-Interface.jl:127-200
     model = pmcmc.DensityModel.diag_gaussian(np.ones(3))
