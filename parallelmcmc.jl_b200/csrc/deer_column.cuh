@@ -183,6 +183,24 @@ struct Col {
   double la;
 };
 
+// g (1 - g) for g = sigmoid(x) (x = log alpha - log u), the slope of the
+// surrogate accept weight in the JVP (MALA.jl:622, 721), as a / (1 + a)^2
+// with a = exp(-|x|): no cancellation in either tail.  It scales only the
+// Jacobian estimate, so FP32 state takes it in FP32; accept decisions use
+// the FP64 log alpha itself.
+template <typename Real>
+__device__ __forceinline__ Real sigmoid_slope(double x) {
+  if constexpr (sizeof(Real) == 4) {
+    const float a = __expf(-fabsf(static_cast<float>(x)));
+    const float inv = __fdividef(1.f, 1.f + a);
+    return a * inv * inv;
+  } else {
+    const double a = exp(-fabs(x));
+    const double inv = 1.0 / (1.0 + a);
+    return a * inv * inv;
+  }
+}
+
 // Forward MALA half (MALA.jl:577-592): gradient, proposal y (Real), gradient
 // at y, and the FP64 log acceptance ratio.  The D/2 log(4 pi eps) constants of
 // the two logq terms cancel exactly and are not formed; y - x - eps g_x is

@@ -244,8 +244,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       Col<Real, QPL> col;
       column_forward<Real, TK, QPL, LPC>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
       const bool acc = logu < col.la;
-      const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
-      const Real gp = static_cast<Real>(gd * (1.0 - gd));
+      const Real gp = sigmoid_slope<Real>(col.la - logu);
       Real A[QPL][4];
       column_jacobian<Real, TK, JAC, QPL, LPC>(P, sm, key, t + P.t_off, iter, acc, gp, col, A);
 #pragma unroll

@@ -83,8 +83,7 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
   la = warp_sum(la) + (P.lpy[t] - P.lpx[t]);
   const double logu = P.logu[t];
   const bool acc = logu < la;
-  const double gd = 1.0 / (1.0 + exp(-(la - logu)));
-  const Real gp = static_cast<Real>(gd * (1.0 - gd));
+  const Real gp = sigmoid_slope<Real>(la - logu);
   Real dla = 0;
 #pragma unroll
   for (int q = 0; q < QPL; ++q)
@@ -221,8 +220,7 @@ __global__ void __launch_bounds__(kThreads)
         Col<Real, QPL> col;
         column_forward<Real, TK, QPL>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
         const bool acc = logu < col.la;
-        const double gd = 1.0 / (1.0 + exp(-(col.la - logu)));
-        const Real gp = static_cast<Real>(gd * (1.0 - gd));
+        const Real gp = sigmoid_slope<Real>(col.la - logu);
         column_jacobian<Real, TK, JAC, QPL>(P, sm, key, t, iter, acc, gp, col, A);
 #pragma unroll
         for (int q = 0; q < QPL; ++q)

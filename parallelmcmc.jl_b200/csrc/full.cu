@@ -221,8 +221,7 @@ __global__ void __launch_bounds__(kThreads)
     column_forward<float, kDiagGauss, 1>(P, sm, key, xcol, static_cast<int>(t), c);
     const double logu = P.logu[t];
     const bool acc = logu < c.la;
-    const double gd = 1.0 / (1.0 + exp(-(c.la - logu)));
-    const float gp = static_cast<float>(gd * (1.0 - gd));
+    const float gp = sigmoid_slope<float>(c.la - logu);
     float s4[4] = {0.f, 0.f, 0.f, 0.f};
     if (4 * lane < D) load4(first ? x0 + 4 * lane : Sold + t * Dp + 4 * lane, s4);
     float v[4], u[4], r[4];
