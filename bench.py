@@ -333,7 +333,7 @@ def run_ours(args):
         nprof = prof["solve_launches"]
         # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload,
         # from the ncu capture summarised in profiles/deer_persist_kernel_aniso_diag_d100.md
-        traffic = 176896
+        traffic = 157184
     else:
         kernel = "deer_sweep_kernel"
         launch_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
