@@ -75,35 +75,6 @@ __device__ __forceinline__ void xi_from_smem(const float* col, int D, float (&n)
   }
 }
 
-// Block-wide maxima of the three partials part[4 c + 0..2] over c < n (every
-// CTA's slot): the same result in every CTA that calls it.
-__device__ __forceinline__ void reduce_partials(const double* part, int n, double* s_red,
-                                                double& a, double& b, double& c) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double x = -INFINITY, y = -INFINITY, z = -INFINITY;
-  for (int i = tid; i < n; i += kThreads) {
-    x = max(x, __ldcg(part + 4 * i));
-    y = max(y, __ldcg(part + 4 * i + 1));
-    z = max(z, __ldcg(part + 4 * i + 2));
-  }
-  x = warp_max(x);
-  y = warp_max(y);
-  z = warp_max(z);
-  __syncthreads();  // s_red may still be read from the previous use
-  if (lane == 0) {
-    s_red[warp] = x;
-    s_red[kWarps + warp] = y;
-    s_red[2 * kWarps + warp] = z;
-  }
-  __syncthreads();
-  a = b = c = -INFINITY;
-  for (int w = 0; w < kWarps; ++w) {
-    a = max(a, s_red[w]);
-    b = max(b, s_red[kWarps + w]);
-    c = max(c, s_red[2 * kWarps + w]);
-  }
-}
-
 }  // namespace
 
 // Two CTAs per SM (at most 128 registers a thread) where that costs no spills:
@@ -127,7 +98,11 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
   // totals of the verification pass, folded in by every CTA as it finishes,
   // and the arrival counter (the grid barriers in between order these resets
   // before every update)
+  // this sweep's maxima max|dS|, max|S| and the non-finite flag, as ordered
+  // bits of non-negative doubles, in two slots by sweep parity (P.part[0..5])
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(P.part);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int i = 0; i < 6; ++i) red[i] = 0ull;
     st->fin_counter = 0;
     st->n_accept = 0;
     st->min_margin_bits = dbits(INFINITY);
@@ -156,7 +131,6 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
   Real* carry0 = incl + static_cast<size_t>(nctas) * Dp;  // S_0 = f(x0)
   Real* Sb = static_cast<Real*>(P.S[0]);                   // last column of every CTA
 
-  double* part = P.part;  // [c][4]: this sweep's max|dS|, max|S|, non-finite flag
   Real* x0s = reinterpret_cast<Real*>(smem_raw + pp.x0);
   {  // start state, zero-padded to Dp
     const Real* src = static_cast<const Real*>(P.x0_src ? P.x0_src : P.x0);
@@ -271,6 +245,9 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       agg_b[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.Bs[(ng - 1) * Dp + d] : Real(0);
     }
     grid.sync();
+    // every CTA has read the previous sweep's slot: clear it for the next sweep
+    if (cta == 0 && tid == 0)
+      for (int i = 0; i < 3; ++i) red[3 * ((iter + 1) & 1) + i] = 0ull;
 
     // ---- state entering every CTA: scan of the group aggregates per coordinate ----
     for (int d = cta; d < D; d += nctas)
@@ -317,7 +294,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
         }
       }
     }
-    // this CTA's partials: plain stores to its own slot (no contended atomics)
+    // this CTA's maxima into the sweep's slot (max is exact in any order; the
+    // CTAs arrive spread over the apply phase, so the atomics rarely meet)
     my_dmax = warp_max(my_dmax);
     my_smax = warp_max(my_smax);
     bad = __any_sync(0xffffffffu, bad);
@@ -327,23 +305,25 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       s_red[2][warp] = bad ? 1.0 : 0.0;
     }
     __syncthreads();
+    unsigned long long* slot = red + 3 * (iter & 1);
     if (tid == 0) {
       double a = 0, b = 0, c = 0;
       for (int w = 0; w < kWarps; ++w)
         a = max(a, s_red[0][w]), b = max(b, s_red[1][w]), c = max(c, s_red[2][w]);
-      part[4 * cta] = a;
-      part[4 * cta + 1] = b;
-      part[4 * cta + 2] = c;
+      atomicMax(slot, dbits(a));
+      atomicMax(slot + 1, dbits(b));
+      if (c != 0.0) atomicMax(slot + 2, 1ull);
     }
     grid.sync();
 
     // ---- convergence test (DEER.jl:567-578), the same in every CTA ----
-    double dmax, smax, nonfinite;
-    reduce_partials(part, nctas, &s_red[0][0], dmax, smax, nonfinite);
+    const double dmax = __longlong_as_double(static_cast<long long>(__ldcg(slot)));
+    const double smax = __longlong_as_double(static_cast<long long>(__ldcg(slot + 1)));
+    const bool nonfinite = __ldcg(slot + 2) != 0ull;
     metric = dmax / (P.tol_abs + P.tol_rel * smax);
     ++iter;
     converged = metric <= 1.0;
-    status = nonfinite != 0.0 ? static_cast<int>(kStNonfinite) : 0;
+    status = nonfinite ? static_cast<int>(kStNonfinite) : 0;
     if (converged || iter >= P.maxiter || status != 0) break;
   }
 
