@@ -250,7 +250,7 @@ __device__ __forceinline__ Real lookback_compose(int tile, int jstar, int d, int
 // one CTA: each thread composes a run of consecutive tiles, a Kogge-Stone scan
 // over the 256 run aggregates in shared memory, then each run is replayed.
 template <typename Real>
-__device__ void carry_scan_tiles(int ntiles, int d, int Dp, const Real* __restrict__ agg_a,
+__device__ void carry_scan_tiles_long(int ntiles, int d, int Dp, const Real* __restrict__ agg_a,
                                  const Real* __restrict__ agg_b, Real s_lo,
                                  Real* __restrict__ carry, Real* sa, Real* sb) {
   const int tid = threadIdx.x;
@@ -289,6 +289,83 @@ __device__ void carry_scan_tiles(int ntiles, int d, int Dp, const Real* __restri
     st = aj * st + bj;
   }
   __syncthreads();
+}
+
+// The same for up to 4 tiles a thread (every persistent and cooperative grid
+// here): each thread keeps its run's aggregates in registers for the replay,
+// and the runs are scanned with warp shuffles, then over the 8 warp totals,
+// with two CTA barriers instead of two a Kogge-Stone step.
+template <typename Real>
+__device__ void carry_scan_tiles(int ntiles, int d, int Dp, const Real* __restrict__ agg_a,
+                                 const Real* __restrict__ agg_b, Real s_lo,
+                                 Real* __restrict__ carry, Real* sa, Real* sb) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr unsigned kAll = 0xffffffffu;
+  constexpr int kRun = 4;  // runs of up to 4 tiles stay in registers for the replay
+  const int K = (ntiles + kThreads - 1) / kThreads;
+  if (K > kRun) {  // more tiles than kRun a thread: the general form
+    carry_scan_tiles_long<Real>(ntiles, d, Dp, agg_a, agg_b, s_lo, carry, sa, sb);
+    return;
+  }
+  const int j0 = min(ntiles, tid * K), j1 = min(ntiles, j0 + K);
+  Real ra[kRun], rb[kRun];
+#pragma unroll
+  for (int k = 0; k < kRun; ++k) {
+    const int j = j0 + k;
+    const bool in = j < j1;
+    ra[k] = in ? __ldcg(agg_a + static_cast<size_t>(j) * Dp + d) : Real(1);
+    rb[k] = in ? __ldcg(agg_b + static_cast<size_t>(j) * Dp + d) : Real(0);
+  }
+  Real a = 1, b = 0;  // this thread's run, composed (identity entries change nothing)
+#pragma unroll
+  for (int k = 0; k < kRun; ++k) {
+    b = ra[k] * b + rb[k];
+    a = ra[k] * a;
+  }
+  // inclusive scan of the runs within the warp (later composed after earlier)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const Real pa = __shfl_up_sync(kAll, a, off), pb = __shfl_up_sync(kAll, b, off);
+    if (lane >= off) {
+      b = a * pb + b;
+      a = a * pa;
+    }
+  }
+  if (lane == 31) {
+    sa[warp] = a;
+    sb[warp] = b;
+  }
+  __syncthreads();
+  if (warp == 0) {  // inclusive scan of the warp totals
+    Real wa = lane < kWarps ? sa[lane] : Real(1), wb = lane < kWarps ? sb[lane] : Real(0);
+#pragma unroll
+    for (int off = 1; off < kWarps; off <<= 1) {
+      const Real pa = __shfl_up_sync(kAll, wa, off), pb = __shfl_up_sync(kAll, wb, off);
+      if (lane >= off) {
+        wb = wa * pb + wb;
+        wa = wa * pa;
+      }
+    }
+    if (lane < kWarps) {
+      sa[kWarps + lane] = wa;
+      sb[kWarps + lane] = wb;
+    }
+  }
+  __syncthreads();
+  // state entering this thread's run: the earlier warps, then the earlier lanes
+  Real st = s_lo;
+  if (warp > 0) st = sa[kWarps + warp - 1] * st + sb[kWarps + warp - 1];
+  const Real la = __shfl_up_sync(kAll, a, 1), lb = __shfl_up_sync(kAll, b, 1);
+  if (lane > 0) st = la * st + lb;
+#pragma unroll
+  for (int k = 0; k < kRun; ++k) {
+    const int j = j0 + k;
+    if (j < j1) {
+      carry[static_cast<size_t>(j) * Dp + d] = st;
+      st = ra[k] * st + rb[k];
+    }
+  }
+  __syncthreads();  // sa / sb are read again by the caller's next use
 }
 
 }  // namespace pmcmc
