@@ -1634,9 +1634,9 @@ int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.X32, x32.data(), 4 * N * Dp, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.y64, y, 8 * N, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->lg.y32, y32.data(), 4 * N, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && D <= 256) {
-    // FP16 hi + lo operands for the tensor-core pass
-    const int64_t Dk = D <= 128 ? 128 : 256;
+  if (e == cudaSuccess && D <= 512) {
+    // FP16 hi + lo operands for the tensor-core pass (Dk = 512: its wide variant)
+    const int64_t Dk = D <= 128 ? 128 : D <= 256 ? 256 : 512;
     const int64_t Np = (N + 127) / 128 * 128;
     std::vector<__half> xh(static_cast<size_t>(Np * Dk), __float2half(0.f)), xl(xh);
     for (int64_t n = 0; n < N; ++n)

@@ -529,6 +529,343 @@ __global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
   }
 }
 
+// ---------------------------------------------------------------------------
+// Wide variant, 256 < D <= 512 (Dk = 512): 16 value columns a CTA (plus 16
+// tangent columns) so that B (48 KB) and R fit beside a ring of four X boxes
+// (128 KB).  The eight 64-wide d boxes of a row block pass through the ring:
+// GEMM1 runs over boxes 0-3, then 4-7 as each slot frees; GEMM2 takes the d
+// quarters 2 and 3 from the resident boxes 4-7, then the quarters 0 and 1
+// from boxes 0-3 loaded again.  Per 128-row block this is the FLOPs of the
+// D <= 256 kernel (half the columns, twice the depth) with 12 box loads
+// instead of 8.  Each slot sees three loads and three releases a block, so
+// its two mbarriers stay one phase per use.
+// ---------------------------------------------------------------------------
+constexpr int BTW = 16;          // value columns per CTA (plus BTW tangent columns)
+constexpr int kSlots = 4;        // X boxes resident at a time
+constexpr int kNkbW = 8;         // 64-wide d boxes of Dk = 512
+constexpr uint32_t kBoxBW = 3 * BTW * 128;  // value hi | tangent | value lo rows of a d box
+
+struct LayoutW {
+  uint32_t xh, xl, b, r, bars, total;
+};
+
+__host__ __device__ inline LayoutW layout_wide() {
+  LayoutW L;
+  uint32_t off = 0;
+  L.xh = off;
+  off += kSlots * kBoxX;
+  L.xl = off;
+  off += kSlots * kBoxX;
+  L.b = off;
+  off += kNkbW * kBoxBW;
+  L.r = off;
+  off += kRAtom;  // one 64-column atom: [r hi 16 | s 16 | r lo 16 | unused 16]
+  L.bars = off;
+  off += 256;
+  L.total = off + 1024;
+  return L;
+}
+
+// 4 consecutive FP32 TMEM columns of this warp's 32 lanes, three times, then
+// one wait in the same asm statement.
+__device__ __forceinline__ void tmem_ld4x3(uint32_t ta, uint32_t tb, uint32_t tc, float (&a)[4],
+                                           float (&b)[4], float (&c)[4]) {
+  uint32_t r[12];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%12];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%4, %5, %6, %7}, [%13];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%8, %9, %10, %11}, [%14];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+      : "r"(ta), "r"(tb), "r"(tc)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    a[i] = __uint_as_float(r[i]);
+    b[i] = __uint_as_float(r[4 + i]);
+    c[i] = __uint_as_float(r[8 + i]);
+  }
+}
+
+// 16 consecutive FP32 TMEM columns of this warp's 32 lanes, twice, one wait.
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float (&a)[16],
+                                            float (&b)[16]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, "
+      "%26, %27, %28, %29, %30, %31}, [%33];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(ta), "r"(tb)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    a[i] = __uint_as_float(r[i]);
+    b[i] = __uint_as_float(r[16 + i]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreadsTC, 1)
+    logistic_pass_tc_wide_kernel(const __grid_constant__ CUtensorMap tmXh,
+                                 const __grid_constant__ CUtensorMap tmXl,
+                                 const __grid_constant__ CUtensorMap tmBh,
+                                 const __grid_constant__ CUtensorMap tmBl,
+                                 const __grid_constant__ CUtensorMap tmBt,
+                                 const float* __restrict__ ylab, int64_t N, int64_t T,
+                                 int64_t Dp, float* __restrict__ G, double* __restrict__ lp,
+                                 int has_tangent, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  const LayoutW Ly = layout_wide();
+  unsigned char* sXh = base + Ly.xh;
+  unsigned char* sXl = base + Ly.xl;
+  unsigned char* sB = base + Ly.b;
+  unsigned char* sR = base + Ly.r;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + Ly.bars);
+  uint64_t* bar_b = bars + 0;   // B loaded
+  uint64_t* bar_x = bars + 1;   // [4] slot loaded
+  uint64_t* bar_f = bars + 5;   // [4] the MMAs reading the slot are done
+  uint64_t* bar_l = bars + 9;   // GEMM1 done (L ready; also GEMM2 of the block before: R free)
+  uint64_t* bar_r = bars + 10;  // epilogue wrote R (32 kEpi arrivals)
+  uint64_t* bar_g = bars + 11;  // GEMM2 of the block done (G final after the last block)
+  uint64_t* bar_z = bars + 12;  // teardown drain
+  __shared__ uint32_t s_tmem;
+  constexpr int BH = BTW / kParts;  // 4 value columns a thread
+  __shared__ double s_red[kEpi][BH];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = static_cast<int64_t>(blockIdx.x) * BTW;
+  const int nblocks = static_cast<int>((N + BN - 1) / BN);
+  const bool has_g = has_tangent != 0;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 13; ++i) mbar_init(bars + i, i == 10 ? 32 * kEpi : 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kProd) tmem_alloc(&s_tmem, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  // L: columns [0, 48) = value (hi*hi + lo*hi) | tangent | value hi*lo;
+  // G quarter q: columns [64 (q + 1), 64 (q + 1) + 48), the same three parts.
+  const uint32_t tL = tmem;
+  auto tG = [&](int q) { return tmem + 64u * static_cast<uint32_t>(q + 1); };
+
+  if (warp == kProd) {
+    if (lane == 0) {
+      bool ok = true;
+      uint32_t xph = 0, fph = 0;  // phase bit of each slot's two barriers
+      const uint32_t i1_all = idesc_f16(128, 3 * BTW, false, false);
+      const uint32_t i1_v = idesc_f16(128, BTW, false, false);
+      const uint32_t i2_all = idesc_f16(128, 3 * BTW, true, true);
+      const uint32_t i2_v = idesc_f16(128, BTW, true, true);
+      auto wait_x = [&](int s) {
+        const bool r = mbar_wait(bar_x + s, (xph >> s) & 1u, err);
+        xph ^= 1u << s;
+        return r;
+      };
+      auto wait_f = [&](int s) {
+        const bool r = mbar_wait(bar_f + s, (fph >> s) & 1u, err);
+        fph ^= 1u << s;
+        return r;
+      };
+      auto load_box = [&](int s, int box, int nb) {
+        mbar_expect_tx(bar_x + s, 2 * kBoxX);
+        tma_2d(sXh + s * kBoxX, &tmXh, box * 64, nb * BN, bar_x + s);
+        tma_2d(sXl + s * kBoxX, &tmXl, box * 64, nb * BN, bar_x + s);
+      };
+      // GEMM1 over the box in slot s: L += Xh [Bh | Bt | Bl] + Xl Bh
+      auto gemm1 = [&](int s, int box) {
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          const uint64_t ah = sdesc(su32(sXh + s * kBoxX) + ks * 32, 16, 1024, 2);
+          const uint64_t al = sdesc(su32(sXl + s * kBoxX) + ks * 32, 16, 1024, 2);
+          const uint64_t bb = sdesc(su32(sB + box * kBoxBW) + ks * 32, 16, 1024, 2);
+          mma_f16(tL, ah, bb, i1_all, (box | ks) != 0);
+          mma_f16(tL, al, bb, i1_v, 1);
+        }
+      };
+      // GEMM2 for d quarter q from the boxes in slots 2p, 2p + 1
+      auto gemm2 = [&](int q, int p, int nb) {
+        if (!has_g) return;
+#pragma unroll
+        for (int kn = 0; kn < BN / 16; ++kn) {
+          const uint64_t ah = sdesc(su32(sXh + 2 * p * kBoxX) + kn * 2048, kBoxX, 1024, 2);
+          const uint64_t al = sdesc(su32(sXl + 2 * p * kBoxX) + kn * 2048, kBoxX, 1024, 2);
+          const uint64_t br = sdesc(su32(sR) + kn * 2048, kRAtom, 1024, 2);
+          const uint32_t acc = (nb > 0 || kn > 0) ? 1u : 0u;
+          mma_f16(tG(q), ah, br, i2_all, acc);
+          mma_f16(tG(q), al, br, i2_v, 1);
+        }
+      };
+      mbar_expect_tx(bar_b, kNkbW * kBoxBW);
+      for (int kb = 0; kb < kNkbW; ++kb) {
+        unsigned char* b = sB + kb * kBoxBW;
+        tma_2d(b, &tmBh, kb * 64, static_cast<int>(t0), bar_b);
+        tma_2d(b + BTW * 128, has_tangent ? &tmBt : &tmBh, kb * 64, static_cast<int>(t0), bar_b);
+        tma_2d(b + 2 * BTW * 128, &tmBl, kb * 64, static_cast<int>(t0), bar_b);
+      }
+      ok = mbar_wait(bar_b, 0, err);
+      if (ok)
+        for (int s = 0; s < kSlots; ++s) load_box(s, s, 0);
+      for (int nb = 0; nb < nblocks && ok; ++nb) {
+        // GEMM1, boxes 0-3
+        for (int s = 0; s < kSlots && ok; ++s) {
+          if (!(ok = wait_x(s))) break;
+          tc_fence_after();
+          gemm1(s, s);
+          mma_commit(bar_f + s);
+        }
+        // boxes 4-7 into the slots as they free, then their GEMM1
+        for (int s = 0; s < kSlots && ok; ++s) {
+          if (!(ok = wait_f(s))) break;
+          load_box(s, kSlots + s, nb);
+        }
+        for (int s = 0; s < kSlots && ok; ++s) {
+          if (!(ok = wait_x(s))) break;
+          tc_fence_after();
+          gemm1(s, kSlots + s);
+        }
+        if (!ok) break;
+        mma_commit(bar_l);
+        if (!(ok = mbar_wait(bar_r, nb & 1, err))) break;
+        tc_fence_after();
+        // GEMM2, quarters 2 and 3 from the resident boxes 4-7
+        for (int p = 0; p < 2; ++p) {
+          gemm2(2 + p, p, nb);
+          mma_commit(bar_f + 2 * p);
+          mma_commit(bar_f + 2 * p + 1);
+        }
+        // boxes 0-3 again, then quarters 0 and 1
+        for (int s = 0; s < kSlots && ok; ++s) {
+          if (!(ok = wait_f(s))) break;
+          load_box(s, s, nb);
+        }
+        for (int p = 0; p < 2 && ok; ++p) {
+          if (!(ok = wait_x(2 * p)) || !(ok = wait_x(2 * p + 1))) break;
+          tc_fence_after();
+          gemm2(p, p, nb);
+          mma_commit(bar_f + 2 * p);
+          mma_commit(bar_f + 2 * p + 1);
+        }
+        if (!ok) break;
+        mma_commit(bar_g);
+        // the next block's boxes 0-3
+        if (nb + 1 < nblocks)
+          for (int s = 0; s < kSlots && ok; ++s) {
+            if (!(ok = wait_f(s))) break;
+            load_box(s, s, nb + 1);
+          }
+      }
+      if (!ok) atomicExch(err, 1);
+      // drain every MMA this thread issued before TMEM is released
+      mma_commit(bar_z);
+      if (!mbar_wait(bar_z, 0, err)) atomicExch(err, 1);
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: thread = TMEM lane = data row; warp part = 4 value columns ----
+    const int quarter = warp & 3, part = warp >> 2;  // columns [4 part, 4 part + 4)
+    const int row = quarter * 32 + lane;
+    const uint32_t lane_off = static_cast<uint32_t>(quarter * 32) << 16;
+    float ls[BH], lc[BH];
+#pragma unroll
+    for (int t = 0; t < BH; ++t) ls[t] = lc[t] = 0.f;
+    bool ok = true;
+    float y_next = row < N ? __ldg(ylab + row) : 0.f;
+    for (int nb = 0; nb < nblocks; ++nb) {
+      const int64_t n = static_cast<int64_t>(nb) * BN + row;
+      const bool valid = n < N;
+      const float yn = y_next;
+      if (n + BN < N) y_next = __ldg(ylab + n + BN);
+      if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
+      tc_fence_after();
+      float v[BH], vl[BH], w[BH];
+      tmem_ld4x3(tL + lane_off + BH * part, tL + lane_off + 2 * BTW + BH * part,
+                 tL + lane_off + BTW + BH * part, v, vl, w);
+      float r[BH], sv[BH];
+#pragma unroll
+      for (int t = 0; t < BH; ++t) {
+        const float l = v[t] + vl[t];
+        const float e = __expf(-fabsf(l));
+        const float inv = __fdividef(1.f, 1.f + e);
+        const float p = l >= 0.f ? inv : e * inv;
+        r[t] = valid ? yn - p : 0.f;
+        sv[t] = (valid && has_tangent) ? p * (1.f - p) * w[t] : 0.f;
+        if (valid) {
+          const float y = (yn * l - (fmaxf(l, 0.f) + log1p_unit(e))) - lc[t];
+          const float sum = ls[t] + y;
+          lc[t] = (sum - ls[t]) - y;
+          ls[t] = sum;
+        }
+      }
+      if (has_g) {
+        uint32_t wh[2], wl[2], ws[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const float h0 = split_hi(r[2 * q]), h1 = split_hi(r[2 * q + 1]);
+          wh[q] = half2_bits(h0, h1);
+          wl[q] = half2_bits(r[2 * q] - h0, r[2 * q + 1] - h1);
+          ws[q] = half2_bits(sv[2 * q], sv[2 * q + 1]);
+        }
+        // 8-column chunks: r hi 0-1, s 2-3, r lo 4-5; this part's half chunk
+        unsigned char* rrow = sR + row * 128 + (part & 1) * 8;
+        const int sw = row & 7, c = part >> 1;
+        *reinterpret_cast<uint2*>(rrow + ((c ^ sw) << 4)) = make_uint2(wh[0], wh[1]);
+        *reinterpret_cast<uint2*>(rrow + (((2 + c) ^ sw) << 4)) = make_uint2(ws[0], ws[1]);
+        *reinterpret_cast<uint2*>(rrow + (((4 + c) ^ sw) << 4)) = make_uint2(wl[0], wl[1]);
+        fence_async_smem();
+      }
+      tc_fence_before();
+      mbar_arrive(bar_r);
+    }
+    if (ok && has_g && mbar_wait(bar_g, (nblocks - 1) & 1, err)) {
+      tc_fence_after();
+      // part q reads d quarter q of G: value (+ its hi*lo part) and tangent
+      const int q = part;
+      float g[16], gl[16], gt[16], unused[16];
+      tmem_ld16x2(tG(q) + lane_off, tG(q) + lane_off + 2 * BTW, g, gl);
+      tmem_ld16x2(tG(q) + lane_off + BTW, tG(q) + lane_off + BTW, gt, unused);
+      const int64_t d = 128 * q + row;
+      if (d < Dp) {
+#pragma unroll
+        for (int t = 0; t < BTW; ++t)
+          if (t0 + t < T) {
+            G[(t0 + t) * Dp + d] = g[t] + gl[t];
+            G[(T + t0 + t) * Dp + d] = gt[t];
+          }
+      }
+    } else if (!ok) {
+      atomicExch(err, 1);
+    }
+#pragma unroll
+    for (int t = 0; t < BH; ++t) {
+      const double sum = warp_sum(static_cast<double>(ls[t]) - static_cast<double>(lc[t]));
+      if (lane == 0) s_red[warp][t] = sum;
+    }
+    asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpi) : "memory");
+    if (threadIdx.x < BTW && t0 + threadIdx.x < T) {
+      const int t = threadIdx.x, hh = t / BH, tt = t % BH;
+      double a = 0.0;
+      for (int q = 0; q < 4; ++q) a += s_red[4 * hh + q][tt];
+      lp[t0 + t] = a;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kProd) tmem_dealloc(tmem, 512);
+}
+
 // Bound check of the mbarrier wait used by the tensor-core pass: one thread
 // initialises a barrier that expects one arrival, nobody arrives, and the
 // bounded wait on phase 0 gives up after kWaitCycles; err[0] = 1 then.
@@ -609,6 +946,20 @@ int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const 
       !make_map(&mBh, Bh, T, Dk, tc::BT) || !make_map(&mBl, Bl, T, Dk, tc::BT) ||
       !make_map(&mBt, Bt, T, Dk, tc::BT))
     return 3;
+  if (Dk == 512) {  // 256 < D <= 512: the wide variant, 16 value columns a CTA
+    CUtensorMap wBh, wBl, wBt;
+    if (!make_map(&wBh, Bh, T, Dk, tc::BTW) || !make_map(&wBl, Bl, T, Dk, tc::BTW) ||
+        !make_map(&wBt, Bt, T, Dk, tc::BTW))
+      return 3;
+    const uint32_t smem = tc::layout_wide().total;
+    if (raise_smem_limit(reinterpret_cast<const void*>(tc::logistic_pass_tc_wide_kernel), smem) !=
+        cudaSuccess)
+      return 3;
+    const int grid = static_cast<int>((T + tc::BTW - 1) / tc::BTW);
+    tc::logistic_pass_tc_wide_kernel<<<grid, tc::kThreadsTC, smem, s>>>(
+        mXh, mXl, wBh, wBl, wBt, X.y32, X.N, T, X.Dp, G, lp, mode != 2 ? 1 : 0, err);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+  }
   const int nkb = static_cast<int>(Dk / 64);
   const tc::Layout Ly = tc::layout(nkb);
   raise_smem_limit(reinterpret_cast<const void*>(tc::logistic_pass_tc_kernel), tc::layout(4).total);

@@ -457,7 +457,9 @@ def _logistic_problem(N, D, seed):
 @pytest.mark.parametrize("dtype,exec_,N,D,T", [
     (np.float64, "plain", 300, 12, 256), (np.float32, "plain", 300, 12, 256),
     (np.float32, "fused", 300, 12, 256),     # tensor-core pass, one accumulator half
-    (np.float32, "fused", 777, 200, 96)])    # two halves, padded rows, partial column tile
+    (np.float32, "fused", 777, 200, 96),     # two halves, padded rows, partial column tile
+    (np.float32, "fused", 650, 300, 72),     # wide pass (D > 256): X through the box ring
+    (np.float32, "fused", 400, 512, 40)])    # wide pass at its largest D
 def test_logistic_matches_sequential(h, dtype, exec_, N, D, T):
     eps = 0.02
     X, y = _logistic_problem(N, D, 31)
@@ -470,7 +472,7 @@ def test_logistic_matches_sequential(h, dtype, exec_, N, D, T):
     Xi, u = O.tape(8, 0, D, T)
     S_seq, acc_seq, _ = O.mala_sequential(tg, eps, np.zeros(D), Xi, u)
     assert info["converged"], info
-    assert bool(info["path"] & 8) == (exec_ == "fused" and dtype == np.float32 and D <= 256)
+    assert bool(info["path"] & 8) == (exec_ == "fused" and dtype == np.float32 and D <= 512)
     assert np.array_equal(acc, acc_seq)
     # converged to tol_rel = 1e-7: FP64 state sits within ~1e-6 of the fixed point
     assert trace_err(S, S_seq) <= (1e-6 if dtype == np.float64 else 1e-5)
