@@ -597,6 +597,15 @@ def run_fleet(args):
     pmcmc.fleet_solve(chains, workers=1, handle=h, errors="report")
     torch.cuda.synchronize()
     serial = time.perf_counter() - t0
+    # plain per-chain FP32 GPU DEER (unfused kernels, cuBLAS FP32 contractions, host
+    # convergence test every iteration), the same chains one at a time, one run
+    import dataclasses
+    plain_chains = [(m, dataclasses.replace(smp, exec="plain"), *rest)
+                    for m, smp, *rest in chains]
+    t0 = time.perf_counter()
+    pres = pmcmc.fleet_solve(plain_chains, workers=1, handle=h, errors="report")
+    torch.cuda.synchronize()
+    plain_t = time.perf_counter() - t0
     acc = [float(np.mean(r[3])) for r in res]
     iters = [r[1]["iters"] for r in res]
     best = min(times)
@@ -621,6 +630,11 @@ def run_fleet(args):
                        "nonfinite": [i for i, r in enumerate(res) if r[1]["status"] == 4]},
             "one_chain_at_a_time": {"value": total_T / serial, "unit": "samples/s",
                                     "speedup_fleet": serial / best},
+            "plain_gpu_per_chain": {"value": total_T / plain_t, "unit": "samples/s",
+                                    "speedup_fleet_over_plain": plain_t / best,
+                                    "converged": sum(r[1]["converged"] for r in pres),
+                                    "newton_iters_median": statistics.median(
+                                        r[1]["iters"] for r in pres)},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
