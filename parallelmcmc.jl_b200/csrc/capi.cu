@@ -598,7 +598,8 @@ int run_fused(pmcmc_handle* h, const SweepKernels& k, bool coop, const DevParams
 
 // One DEER block as one cooperative launch of the persistent solve kernel
 // (tape, every sweep and the verification pass; deer_persist.cu).
-int run_persist(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t smem) {
+int run_persist(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size_t smem,
+                int64_t nblk) {
   CK(raise_smem_limit(k.persist, smem));
   DevParams Pv = P;  // by value in the launch
   void* args[] = {&Pv, &h->d_state};
@@ -614,7 +615,11 @@ int run_persist(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, size
     CK(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
     h->prof.solve_launches += 1;
     h->prof.solve_ms += ms;
-    h->prof.solve_sweeps += h->h_state->iter;
+    if (nblk > 1) {  // the blocks' states are in the pinned ring
+      for (int64_t b = 0; b < nblk; ++b) h->prof.solve_sweeps += P.st_host[b].iter;
+    } else {
+      h->prof.solve_sweeps += h->h_state->iter;
+    }
   }
   return PMCMC_OK;
 }
@@ -1183,6 +1188,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   // Several blocks: each block's state goes to a pinned ring, read after the last
   // block, so the blocks run back to back with no host round trip between them.
   const bool defer = nblocks > 1;
+  // Device outputs of several blocks on the persistent path: one launch solves
+  // them all, the kernel looping over the blocks (a grid barrier between blocks
+  // instead of a kernel boundary).
+  const bool batch = persist && mem == PMCMC_MEM_DEVICE && nblocks > 1;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
                                use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr,
                                false, pipe);
@@ -1290,6 +1299,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     P.x0 = ws + ((b & 1) ? L.x0b : L.x0a);
     P.x_next = ws + ((b & 1) ? L.x0a : L.x0b);
     P.ncols_out = nkeep;
+    if (batch) {  // every block of the call in this launch; ncols_out: the last block's
+      P.nblk = nblocks;
+      P.ncols_out = N - (nblocks - 1) * T;
+    }
     if (persist) {
       P.x0_src = (b == 0 && mem == PMCMC_MEM_DEVICE) ? x0 : P.x0;
       P.st_host = defer ? h->h_states + b : h->h_state;  // written by the kernel
@@ -1310,7 +1323,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
          : full   ? run_full(h, k, fplan, P, eigen_view(P, tg, ws, L), F, sp_fin.total,
                              fin_grid, init_grid)
          : plain   ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
-         : persist ? run_persist(h, k, P, persist_smem(f64, Dp, TT, dense).total)
+         : persist ? run_persist(h, k, P, persist_smem(f64, Dp, TT, dense).total,
+                                 batch ? nblocks : 1)
                    : run_fused(h, k, tp.coop, P, sp_sweep.total, sp_fin.total, fin_grid,
                                init_grid);
     if (rc) return rc;
@@ -1331,6 +1345,10 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
       if (pipe) CK(cudaEventRecord(h->ev_copy[slot], cs));
     }
     nsteps += nkeep;
+    if (batch) {  // the launch solved every block
+      nsteps = N;
+      break;
+    }
     if (defer) {  // block states are read after the last block
       if (!persist)
         CK(cudaMemcpyAsync(h->h_states + b, h->d_state, sizeof(DevState),

@@ -67,6 +67,11 @@ struct DevParams {
   double* part;         // [2 * ntiles * 4] per-CTA partial reductions
   const void* x0_src;   // start state as given (D entries, unpadded), or nullptr: use x0
   DevState* st_host;    // pinned host copy of the final state (nullptr: none)
+  // blocks solved back to back in one persistent launch (0 or 1: one).  Block b
+  // is tape block `block + b`, starts from block b - 1's x_next, writes its
+  // rows at S_out + b T D (logp, accept: + b T) and its state to st_host[b];
+  // ncols_out is then the last block's kept columns (the others keep T).
+  int64_t nblk;
 };
 
 struct DevState {
