@@ -222,7 +222,9 @@ __device__ __forceinline__ void load_xi(const DevParams& P, int64_t t, float (&n
   }
 }
 
-template <typename Real, int TK, int QPL, int LPC = 32>
+// kReduce = false leaves c.la as this lane's partial sum, for a caller that
+// reduces it together with its own per-lane sums.
+template <typename Real, int TK, int QPL, int LPC = 32, bool kReduce = true>
 __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Real>& sm,
                                                const TapeKey& key, const Real* xcol, int t,
                                                Col<Real, QPL>& c,
@@ -354,7 +356,7 @@ __device__ __forceinline__ void column_forward(const DevParams& P, const Smem<Re
     }
     __syncwarp();
   }
-  c.la = seg_sum<LPC>(la);
+  c.la = kReduce ? seg_sum<LPC>(la) : la;
 }
 
 // Dense HVP quad: out = -P v (v written to the warp's Real vector first).

@@ -372,9 +372,9 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       float xic[QPL][4];
       xi_from_smem<QPL, LPC>(xis + c * Dp, D, xic);
       Col<Real, QPL> col;
-      column_forward<Real, TK, QPL, LPC>(P, sm, key, xcol, static_cast<int>(t), col, xic);
+      // log alpha reduced below with the log density and the defect (one pass)
+      column_forward<Real, TK, QPL, LPC, false>(P, sm, key, xcol, static_cast<int>(t), col, xic);
       const double logu = lus[c];
-      const bool acc = logu < col.la;
       const bool out = valid && t < ncols_out;
       // the recursion defect max|S_t - f_t| for both outcomes, selected after the
       // reductions (which then run alongside the log-density's)
@@ -416,10 +416,12 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       }
 #pragma unroll
       for (int o = LPC / 2; o > 0; o >>= 1) {
+        col.la += __shfl_xor_sync(0xffffffffu, col.la, o);
         lp += __shfl_xor_sync(0xffffffffu, lp, o);
         dx = max(dx, __shfl_xor_sync(0xffffffffu, dx, o));
         dy = max(dy, __shfl_xor_sync(0xffffffffu, dy, o));
       }
+      const bool acc = logu < col.la;
       if (valid && lq == 0) {
         if (out) {
           if (logp_out) logp_out[t] = static_cast<Real>(lp);
