@@ -156,8 +156,11 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       for (int e = 0; e < 4; ++e)
         if (4 * q + e >= D) n[e] = 0.f;
       store4(xis + 4 * q, n);
-      if (q == 0) lus[0] = log(static_cast<double>(tape_u(key, tg)));
     }
+    // log u of the columns t0 .. t0 + ng (the CTA's own and its scan group's), in
+    // FP64, one column a thread: the evaluation reads them from shared memory
+    for (int c = tid; c <= ng; c += kThreads)
+      lus[c] = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t0 + c + P.t_off))));
     __syncthreads();
     for (int i = tid; i < ncols * (Dp / 4); i += kThreads) {
       const int nq = Dp / 4, c = i / nq, k = 4 * (i - c * nq);
@@ -217,9 +220,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
               for (int e = 0; e < 4; ++e) xic[q][e] = 0.f;
             }
           }
-          const double lu = lq == 0 ? log(static_cast<double>(tape_u(key, tg))) : 0.0;
-          logu = __shfl_sync(0xffffffffu, lu, half * LPC);
-          if (valid && lq == 0) lus[c + 1] = logu;
+          logu = lus[c + 1];
         } else {
           xi_from_smem<QPL, LPC>(xis + (c + 1) * Dp, D, xic);
           logu = lus[c + 1];
