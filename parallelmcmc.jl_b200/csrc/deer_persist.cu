@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     const Real dmp = static_cast<Real>(P.damping), omd = static_cast<Real>(1.0 - P.damping);
     const bool undamped = P.damping == 1.0;
     int iter = 0, converged = 0, status = 0;
+    Real sprev = 0;
     double metric = 0.0;
     for (;;) {
       // ---- evaluate the scan group: column t0 + c + 1 from S_{t0 + c} ----
@@ -325,6 +326,9 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
         if (c != 0.0) atomicMax(slot + 2, 1ull);
       }
       grid.sync();
+      // S_{t0 - 1} (the previous CTA's last column) for the verification, should
+      // this sweep be the last: its load overlaps the test's
+      if (cta > 0 && tid < Dp) sprev = __ldcg(Sb + (t0 - 1) * Dp + tid);
 
       // ---- convergence test (DEER.jl:567-578), the same in every CTA ----
       const double dmax = __longlong_as_double(static_cast<long long>(__ldcg(slot)));
@@ -340,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     // ---- verification pass and outputs on the CTA's columns ----
     // S_{t0 - 1}, the previous CTA's last column, into shared memory
     for (int d = tid; d < Dp; d += kThreads)
-      sm.carry[d] = cta == 0 ? x0s[d] : __ldcg(Sb + (t0 - 1) * Dp + d);
+      sm.carry[d] = cta == 0 ? x0s[d] : d == tid ? sprev : __ldcg(Sb + (t0 - 1) * Dp + d);
     // the CTA's rows of S_out (row t = column t, D entries) in one coalesced copy
     {
       const int64_t nrows = imin64(ncols, ncols_out - t0);
