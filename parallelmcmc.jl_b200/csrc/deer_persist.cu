@@ -140,10 +140,10 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
       st->min_margin_bits = dbits(INFINITY);
       st->max_defect_bits = 0;
     }
-    {  // start state, zero-padded to Dp: the call's x0, or the previous block's last column
-      const Real* src = static_cast<const Real*>(bi > 0 ? P.x_next : P.x0_src ? P.x0_src : P.x0);
-      for (int d = tid; d < Dp; d += kThreads) x0s[d] = d < D ? src[d] : Real(0);
-    }
+    // start state, zero-padded to Dp: the call's x0, or the previous block's last
+    // column; loaded here, stored to shared memory after the tape work below
+    const Real* x0src = static_cast<const Real*>(bi > 0 ? P.x_next : P.x0_src ? P.x0_src : P.x0);
+    const Real x0r = tid < D ? x0src[tid] : Real(0);
 
     // ---- tape (interface.jl:334-358) of column t0 here; columns t0 + 1 ..
     // t0 + ncols are drawn by the first sweep's evaluation, which uses them first ----
@@ -161,6 +161,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     // FP64, one column a thread: the evaluation reads them from shared memory
     for (int c = tid; c <= ng; c += kThreads)
       lus[c] = log(static_cast<double>(tape_u(key, static_cast<uint32_t>(t0 + c + P.t_off))));
+    for (int d = tid; d < Dp; d += kThreads)
+      x0s[d] = d == tid ? x0r : d < D ? x0src[d] : Real(0);
     __syncthreads();
     for (int i = tid; i < ncols * (Dp / 4); i += kThreads) {
       const int nq = Dp / 4, c = i / nq, k = 4 * (i - c * nq);
