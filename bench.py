@@ -528,6 +528,21 @@ def run_secondary(args):
                        "accept_rate": acc_rate, "path": infos[-1].as_dict()["path_names"]},
             "clocks": clk.summary()}
     if logistic:
+        # plain FP32 GPU DEER on the first timed block: unfused kernels, cuBLAS FP32
+        # contractions, the convergence test on the host after every iteration
+        import dataclasses
+        plain = dataclasses.replace(sampler, exec="plain")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record(stream)
+        pinfo = solve_dev(plain, 1000)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        pms = e0.elapsed_time(e1)
+        line["plain_gpu"] = {"value": T / (pms / 1e3), "unit": "samples/s", "block": 1000,
+                             "newton_iters": pinfo.iters, "converged": bool(pinfo.converged),
+                             "fused_newton_iters_same_block": infos[0].iters,
+                             "speedup_fused_over_plain": value / (T / (pms / 1e3))}
         N = meta.get("N_rows", 10_000)
         pass_ms = prof["pass_ms"] / max(1, prof["pass_launches"])
         flops = 8.0 * N * D * T  # two GEMMs of 2 N D (2T) per contraction pass

@@ -90,7 +90,9 @@ typedef struct {
   double metric;       /* max|dS| / (tol_abs + tol_rel max|S|), FP64 */
   int64_t n_accept;    /* accepted proposals on the returned trajectory */
   double min_margin;   /* min_t |logalpha_t - log u_t| (FP64) */
-  double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory */
+  double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory; NaN for
+                          the logistic target, whose accept flags and margins are those of
+                          the last sweep (f is not evaluated again at the returned S) */
   int32_t status;      /* pmcmc_status of the device work */
   int32_t path;        /* PMCMC_PATH_* bits: which kernels ran */
 } pmcmc_info;
