@@ -145,17 +145,21 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     const Real* x0src = static_cast<const Real*>(bi > 0 ? P.x_next : P.x0_src ? P.x0_src : P.x0);
     const Real x0r = tid < D ? x0src[tid] : Real(0);
 
-    // ---- tape (interface.jl:334-358) of column t0 here; columns t0 + 1 ..
-    // t0 + ncols are drawn by the first sweep's evaluation, which uses them first ----
+    // ---- tape (interface.jl:334-358) of the CTA's columns, drawn once a block ----
     const TapeKey key(P.seed, P.block + static_cast<uint64_t>(bi));
-    for (int q = tid; q < Dp / 4; q += kThreads) {
-      const uint32_t tg = static_cast<uint32_t>(t0 + P.t_off);
-      float n[4];
-      tape_xi4(key, static_cast<uint32_t>(q), tg, n);
+    // the tape of columns t0 .. t0 + ng (the CTA's own and its scan group's), one
+    // (column, quad) pair a thread at a time: every lane busy, however D splits
+    {
+      const int nq = Dp / 4;
+      for (int i = tid; i < (ng + 1) * nq; i += kThreads) {
+        const int c = i / nq, q = i - c * nq;
+        float n[4];
+        tape_xi4(key, static_cast<uint32_t>(q), static_cast<uint32_t>(t0 + c + P.t_off), n);
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (4 * q + e >= D) n[e] = 0.f;
-      store4(xis + 4 * q, n);
+        for (int e = 0; e < 4; ++e)
+          if (4 * q + e >= D) n[e] = 0.f;
+        store4(xis + c * Dp + 4 * q, n);
+      }
     }
     // log u of the columns t0 .. t0 + ng (the CTA's own and its scan group's), in
     // FP64, one column a thread: the evaluation reads them from shared memory
@@ -205,29 +209,8 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
         const int c = valid ? cb + half : cb;
         const int t = static_cast<int>(t0 + c + 1);
         float xic[QPL][4];
-        double logu;
-        if (iter == 0) {
-          // first use of column t's tape: drawn here, kept in shared memory
-          const uint32_t tg = static_cast<uint32_t>(t + P.t_off);
-#pragma unroll
-          for (int q = 0; q < QPL; ++q) {
-            const int j = lq + LPC * q;
-            if (4 * j < D) {
-              tape_xi4(key, static_cast<uint32_t>(j), tg, xic[q]);
-#pragma unroll
-              for (int e = 0; e < 4; ++e)
-                if (4 * j + e >= D) xic[q][e] = 0.f;
-              if (valid) store4(xis + (c + 1) * Dp + 4 * j, xic[q]);
-            } else {
-#pragma unroll
-              for (int e = 0; e < 4; ++e) xic[q][e] = 0.f;
-            }
-          }
-          logu = lus[c + 1];
-        } else {
-          xi_from_smem<QPL, LPC>(xis + (c + 1) * Dp, D, xic);
-          logu = lus[c + 1];
-        }
+        xi_from_smem<QPL, LPC>(xis + (c + 1) * Dp, D, xic);
+        const double logu = lus[c + 1];
         Col<Real, QPL> col;
         column_forward<Real, TK, QPL, LPC>(P, sm, key, sm.Xs + c * Dp, t, col, xic);
         const bool acc = logu < col.la;
