@@ -332,9 +332,9 @@ def run_ours(args):
         min_bytes = 4 * D * T + 5 * T  # S, logp, accept out; S and the tape stay on chip
         nprof = prof["solve_launches"]
         # dram__bytes_read.sum + dram__bytes_write.sum per block, from the ncu capture of
-        # an 8-block launch of this workload (145,408 + 1,515,776 B over 8 blocks),
+        # an 8-block launch of this workload (136,704 + 1,610,240 B over 8 blocks),
         # summarised in profiles/deer_persist_kernel_aniso_diag_d100.md
-        traffic = 207648
+        traffic = 218368
     else:
         kernel = "deer_sweep_kernel"
         launch_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
