@@ -472,7 +472,8 @@ def run_secondary(args):
     lib = L.load()
     logistic = args.workload == "logistic_n10k_d256"
     if logistic:
-        model, sampler, x0, meta = configs.logistic_n10k_d256(T=4096 if args.small else 65536)
+        model, sampler, x0, meta = configs.logistic_n10k_d256(T=4096 if args.small else 65536,
+                                                              D=args.dim)
     else:
         model, sampler, x0, meta = configs.correlated_gauss_d64(T=1024 if args.small else 8192)
         # the sampler's default stopping rule (1e-6 + 1e-5 |S|) allows ~1e-5 relative
@@ -552,7 +553,8 @@ def run_secondary(args):
         except Exception:
             tpk, tsrc = 1590.0, "fallback"
         achieved = flops / (pass_ms / 1e3) / 1e12
-        line["roofline"] = {"bound": "tensor", "kernel": "logistic_pass_tc_kernel (+ mid kernel)",
+        kname = "logistic_pass_tc_wide_kernel" if D > 256 else "logistic_pass_tc_kernel"
+        line["roofline"] = {"bound": "tensor", "kernel": f"{kname} (+ mid kernel)",
                             "achieved": achieved, "peak": tpk, "unit": "TFLOP/s",
                             "frac": achieved / tpk, "peak_source": tsrc,
                             "avg_launch_ms": pass_ms, "alg_flops_per_launch": flops,
@@ -665,6 +667,9 @@ def main():
     ap.add_argument("--workload", default="aniso_diag_d100",
                     choices=["aniso_diag_d100", "logistic_n10k_d256", "corr_gauss_d64_full",
                              "logistic_fleet"])
+    ap.add_argument("--dim", type=int, default=256,
+                    help="logistic workload: dimension D (256 < D <= 512 runs the wide "
+                         "tensor-core pass)")
     ap.add_argument("--small", action="store_true",
                     help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()
