@@ -153,7 +153,12 @@ int pmcmc_deer_solve(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_pa
  * block b, keeps min(T, N - nsteps) columns, next x0 = last kept column.
  * vals_out D x N (dtype), logp_out N (dtype, may be NULL), accept_out N (may be NULL).
  * info accumulates: iters = total sweeps, converged = all blocks converged,
- * metric = worst block metric. */
+ * metric = worst block metric.
+ * The blocks run back to back with no host round trip between them; with device
+ * outputs on the persistent path (Gaussian targets) they are one launch.  A block
+ * that fails (non-finite state) does not stop the blocks after it, whose outputs
+ * are then meaningless; the call returns the first failing block's status and info
+ * counts the blocks up to it. */
 int pmcmc_sample(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
                  const void* x0, uint64_t seed, int64_t N, void* vals_out, void* logp_out,
                  uint8_t* accept_out, int32_t mem, pmcmc_info* info);
