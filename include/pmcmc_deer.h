@@ -90,9 +90,10 @@ typedef struct {
   double metric;       /* max|dS| / (tol_abs + tol_rel max|S|), FP64 */
   int64_t n_accept;    /* accepted proposals on the returned trajectory */
   double min_margin;   /* min_t |logalpha_t - log u_t| (FP64) */
-  double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory; NaN for
-                          the logistic target, whose accept flags and margins are those of
-                          the last sweep (f is not evaluated again at the returned S) */
+  double max_defect;   /* max_t |S_t - f_t(S_{t-1})|_inf of the returned trajectory, from a
+                          verification pass at the returned S (accept flags and margins come
+                          from the same pass); NaN on the plain logistic path
+                          (PMCMC_EXEC_PLAIN), whose flags are those of its last sweep */
   int32_t status;      /* pmcmc_status of the device work */
   int32_t path;        /* PMCMC_PATH_* bits: which kernels ran */
 } pmcmc_info;
@@ -103,6 +104,8 @@ typedef struct {
 #define PMCMC_PATH_TENSOR_CORE 8  /* logistic passes on tcgen05 tensor cores */
 #define PMCMC_PATH_FULL_JACOBIAN 16 /* :full mode (dense Jacobian, eigenbasis chunk scan) */
 #define PMCMC_PATH_PERSISTENT 32  /* whole solve in one cooperative launch, state in shared memory */
+#define PMCMC_PATH_TIE_FP64 64    /* logistic, FP32 state: near-tie accept decisions taken from an
+                                     FP64 evaluation of log alpha in every sweep */
 
 /* ---- handle ------------------------------------------------------------ */
 /* Replaces DEERWorkspace (src/DEER/DEER.jl:47-90): owns all device workspace,

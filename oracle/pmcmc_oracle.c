@@ -339,6 +339,91 @@ void orc_mala_sequential(const orc_target* tg, double eps, const double* x0, con
     }
 }
 
+/* lp(th) and g(th) of the logistic target, with the arithmetic of orc_logp and
+ * orc_grad (bayes_logreg.jl:37-58): every logit sums over i in order, every
+ * gradient entry over n in order, and the log-likelihood terms are added in
+ * row order.  Threads split the rows (logits, terms) and the coordinates
+ * (gradient), which leaves each sum's order, and so its rounding, unchanged. */
+static double logistic_lp_grad(const orc_target* tg, const double* th, double* l, double* term,
+                               double* g, int nth) {
+    const int64_t N = tg->N, D = tg->D;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nth)
+#endif
+    {
+        int me = 0, nt = 1;
+#ifdef _OPENMP
+        me = omp_get_thread_num();
+        nt = omp_get_num_threads();
+#endif
+        const int64_t n0 = N * me / nt, n1 = N * (me + 1) / nt;
+        for (int64_t n = n0; n < n1; ++n) l[n] = 0.0;
+        for (int64_t i = 0; i < D; ++i) {
+            const double* col = tg->X + i * N;
+            const double ti = th[i];
+            for (int64_t n = n0; n < n1; ++n) l[n] += col[n] * ti;
+        }
+        for (int64_t n = n0; n < n1; ++n) {
+            term[n] = tg->y[n] * (-softplus(-l[n])) + (1.0 - tg->y[n]) * (-softplus(l[n]));
+            l[n] = tg->y[n] - sigm(l[n]);
+        }
+#ifdef _OPENMP
+#pragma omp barrier
+#pragma omp for schedule(static)
+#endif
+        for (int64_t i = 0; i < D; ++i) {
+            const double* col = tg->X + i * N;
+            double s = 0;
+            for (int64_t n = 0; n < N; ++n) s += col[n] * l[n];
+            g[i] = s - tg->prior_prec * th[i];
+        }
+    }
+    double s = 0;
+    for (int64_t n = 0; n < N; ++n) s += term[n];
+    double q = 0;
+    for (int64_t i = 0; i < D; ++i) q += th[i] * th[i];
+    return s - 0.5 * tg->prior_prec * q;
+}
+
+/* orc_mala_sequential for the logistic target, with the log density and the
+ * gradient of an accepted proposal carried to the next step (they are the
+ * values at the new state) and the target's sums split over threads as in
+ * logistic_lp_grad: the same results as orc_mala_sequential, bit for bit, in
+ * a time that makes full-size chains (N = 10000, D = 256, T = 65536) a test. */
+void orc_mala_sequential_logistic(const orc_target* tg, double eps, const double* x0,
+                                  const double* Xi, const double* u, int64_t T, double* S,
+                                  int32_t* accepted, double* logalpha, int32_t nthreads) {
+    const int64_t N = tg->N, D = tg->D;
+    int nth = 1;
+#ifdef _OPENMP
+    nth = nthreads > 0 ? nthreads : omp_get_max_threads();
+#endif
+    (void)nthreads;
+    double* buf = (double*)malloc(sizeof(double) * (2 * N + 4 * D));
+    double *l = buf, *term = buf + N, *x = buf + 2 * N, *gx = x + D, *y = gx + D, *gy = y + D;
+    memcpy(x, x0, sizeof(double) * D);
+    double lpx = logistic_lp_grad(tg, x, l, term, gx, nth);
+    const double s2e = sqrt(2 * eps);
+    for (int64_t t = 0; t < T; ++t) {
+        const double* xi = Xi + t * D;
+        for (int64_t i = 0; i < D; ++i) y[i] = x[i] + eps * gx[i] + s2e * xi[i];
+        const double lpy = logistic_lp_grad(tg, y, l, term, gy, nth);
+        const double lq_yx = orc_logq(tg, y, x, gx, eps);
+        const double lq_xy = orc_logq(tg, x, y, gy, eps);
+        const double la = (lpy + lq_xy) - (lpx + lq_yx);
+        const int acc = log(u[t]) < la; /* strict, MALA.jl:404 */
+        if (acc) {
+            memcpy(x, y, sizeof(double) * D);
+            memcpy(gx, gy, sizeof(double) * D);
+            lpx = lpy;
+        }
+        memcpy(S + t * D, x, sizeof(double) * D);
+        if (accepted) accepted[t] = acc;
+        if (logalpha) logalpha[t] = la;
+    }
+    free(buf);
+}
+
 /* Per-column fused forward + surrogate JVP in the batched operation order of
  * mala_step_batched_fwd_and_jvp! (MALA.jl:577-626), identity mass matrix. */
 static void fwd_jvp_col(const orc_target* tg, double eps, const double* x, const double* xi,

@@ -82,6 +82,12 @@ double orc_mala_step(const orc_target* tg, double eps, const double* x, const do
 void orc_mala_sequential(const orc_target* tg, double eps, const double* x0, const double* Xi,
                          const double* u, int64_t T, double* S, int32_t* accepted,
                          double* logalpha);
+/* orc_mala_sequential for the logistic target, the accepted proposal's log density and
+ * gradient carried to the next step, the target's sums split over threads with their
+ * order kept: the same results bit for bit, fast enough for full-size chains. */
+void orc_mala_sequential_logistic(const orc_target* tg, double eps, const double* x0,
+                                  const double* Xi, const double* u, int64_t T, double* S,
+                                  int32_t* accepted, double* logalpha, int32_t nthreads);
 void orc_fwd_and_jvp(const orc_target* tg, double eps, const double* x, const double* xi,
                      double u, const double* v, double* f, double* jv);
 void orc_fwd_and_jvp_batched(const orc_target* tg, double eps, int64_t T, const double* X,

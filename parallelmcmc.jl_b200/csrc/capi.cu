@@ -366,6 +366,7 @@ struct SolveLayout {
   size_t S0, S1, x0a, x0b, flags, agg_a, agg_b, incl, colmax, out_S, out_lp, out_acc;
   size_t pA, pB, al0, be0, al1, be1, red;  // plain path only
   size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
+  size_t la_ref, tie;                                   // logistic: log alpha, near-tie scratch
   size_t xi, logu;
   size_t tcws, Gtc;  // tensor-core logistic path
   size_t fU, fV, fR, facc, fPhi, fbeta, fdin, fpart, eS0, eS1, exi, ex0;  // :full mode
@@ -378,7 +379,7 @@ struct SolveLayout {
 SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool plain,
                    int64_t N = 0, int64_t Tc = 0, size_t tc_bytes = 0,
                    const FullPlan* fp = nullptr, bool adjoint = false,
-                   bool dual_out = false) {
+                   bool dual_out = false, size_t tie_bytes = 0) {
   SolveLayout L{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -424,6 +425,8 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
     L.Bb = take(es * Dp * 2 * Tc);
     L.Lb = take(es * N * 2 * Tc);
     L.Gb = take(es * Dp * 2 * Tc);
+    L.la_ref = take(8 * static_cast<size_t>(T));
+    L.tie = take(tie_bytes);
   }
   if (tc_bytes) {
     L.tcws = take(tc_bytes);
@@ -689,14 +692,29 @@ int run_plain(pmcmc_handle* h, const SweepKernels& k, const DevParams& P, const 
   return PMCMC_OK;
 }
 
+// Near-tie band of the FP64 decisions of the logistic target and the most
+// columns one refinement recomputes (logistic_tie.cu).  The tensor-core
+// log alpha is off by up to ~1e-4; columns inside 1e-3 (about 60 of 65536 at
+// N = 10000, D = 256) are decided in FP64.
+constexpr float kTieBand = 1e-3f;
+constexpr int kTieMax = 256;
+int tie_kmax(int64_t T) { return static_cast<int>(std::min<int64_t>(kTieMax, T)); }
+
 // One DEER block for the logistic target: per Newton iteration two GEMM
 // passes (pass 1 at [x_bar | z], pass 2 at [y | w]) feed the fused
-// finish + scan sweep kernel; then a logp pass over the returned trajectory.
+// finish + scan sweep kernel.  On the fused FP32 path the columns near a tie
+// are decided in FP64 before the sweep (`refine`).  Then, on the fused path, a
+// verification pass at the returned trajectory (its passes at x_bar_t =
+// S_{t-1}: accept flags, margins, defect) and a logp pass over it.
 int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k, bool coop,
-                 const DevParams& P, const SolveLayout& L, size_t es, size_t smem_sweep,
-                 int fin_grid, int init_grid, int64_t Tc, bool use_tc) {
+                 DevParams P, const SolveLayout& L, size_t es, size_t smem_sweep,
+                 int fin_grid, int init_grid, int64_t Tc, bool use_tc, bool plain) {
   unsigned char* ws = h->ws;
   const bool f64 = es == 8;
+  const bool refine = !plain && !f64;
+  double* la_ref = reinterpret_cast<double*>(ws + L.la_ref);
+  const TieBufs tb = lg_tie_carve(ws + L.tie, tg->lg, P.T, tie_kmax(P.T));
+  P.la_ref = refine ? la_ref : nullptr;
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(coop ? k.sweep_coop : k.sweep), smem_sweep));
@@ -743,6 +761,16 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     }
     return pass_impl(mode, lp);
   };
+  auto tie = [&]() -> int {
+    if (lg_tie_refine(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.T, la_ref,
+                      tb, kTieBand))
+      return fail(h, PMCMC_ERR_CUDA, "near-tie refinement failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+    return PMCMC_OK;
+  };
+  // the tensor-core error word travels with the state in every per-sweep copy
+  int* h_err = reinterpret_cast<int*>(h->h_red + 3);
+  *h_err = 0;
   for (int it = 0; it < P.maxiter; ++it) {
     if (pass(0, P.lpx))
       return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
@@ -750,12 +778,18 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     if (pass(1, P.lpy))
       return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
                   cudaGetErrorString(cudaGetLastError()));
+    if (refine) {
+      const int rc = tie();
+      if (rc) return rc;
+    }
     if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
     CK(launch_sweep(coop ? k.sweep_coop : k.sweep, coop, P.ntiles, smem_sweep, sweep_args,
                     h->stream));
     if (h->profiling) CK(cudaEventRecord(h->ev[1], h->stream));
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
                        h->stream));
+    if (use_tc)
+      CK(cudaMemcpyAsync(h_err, tc_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (h->profiling) {
       float ms = 0;
@@ -763,16 +797,30 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
       h->prof.sweep_launches += 1;
       h->prof.sweep_ms += ms;
     }
+    if (*h_err) return fail(h, PMCMC_ERR_TIMEOUT, "tensor-core pass: a bounded wait gave up");
     if (h->h_state->converged || h->h_state->status) break;
+  }
+  if (!plain && !h->h_state->status) {
+    // verification at the returned trajectory: the passes at x_bar_t = S_{t-1},
+    // the near-tie decisions in FP64, then flags, margins and the defect
+    if (pass(0, P.lpx) || pass(1, P.lpy))
+      return fail(h, PMCMC_ERR_CUDA, "logistic verification pass failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+    if (refine) {
+      const int rc = tie();
+      if (rc) return rc;
+    } else {
+      CK(lg_margin(h->stream, f64, h->d_params, h->d_state, P.T, la_ref, tb.mg));
+    }
+    CK(lg_verify(h->stream, f64, h->d_params, h->d_state, P.T, la_ref));
   }
   if (pass(2, P.lpx)) return fail(h, PMCMC_ERR_CUDA, "logistic logp pass failed");
   void* fin_args[] = {&h->d_params, &h->d_state};
   CK(cudaLaunchKernel(k.finalize, dim3(fin_grid), dim3(kThreads), fin_args, 0, h->stream));
   if (use_tc) {
-    int e = 0;
-    CK(cudaMemcpyAsync(&e, tc_err, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h_err, tc_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (e) return fail(h, PMCMC_ERR_TIMEOUT, "tensor-core pass: a bounded wait gave up");
+    if (*h_err) return fail(h, PMCMC_ERR_TIMEOUT, "tensor-core pass: a bounded wait gave up");
   }
   return PMCMC_OK;
 }
@@ -1194,7 +1242,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   const bool batch = persist && mem == PMCMC_MEM_DEVICE && nblocks > 1;
   const SolveLayout L = layout(D, Dp, T, ntiles, es, plain, logistic ? tg->N : 0, Tc,
                                use_tc ? lg_tc_ws_bytes(tg->lg, T) : 0, full ? &fplan : nullptr,
-                               false, pipe);
+                               false, pipe,
+                               logistic ? lg_tie_ws_bytes(tg->lg, T, tie_kmax(T)) : 0);
   rc = ensure_ws(h, L.total);
   if (rc) return rc;
   if (defer) {
@@ -1319,7 +1368,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     // the slot's previous contents (block b - 2) must be copied out first
     if (pipe && b >= 2) CK(cudaStreamWaitEvent(h->stream, h->ev_copy[slot], 0));
     rc = logistic ? run_logistic(h, tg, k, tp.coop, P, L, es, sp_sweep.total, fin_grid,
-                                 init_grid, Tc, use_tc)
+                                 init_grid, Tc, use_tc, plain)
          : full   ? run_full(h, k, fplan, P, eigen_view(P, tg, ws, L), F, sp_fin.total,
                              fin_grid, init_grid)
          : plain   ? run_plain(h, k, P, L, es, sp_fin.total, fin_grid, init_grid)
@@ -1391,13 +1440,16 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   }
   agg.status = status;
   if (nblocks == 1) fill_info(states[0], &agg);
+  // the plain logistic path keeps the last sweep's flags and verifies nothing
+  if (logistic && plain) agg.max_defect = NAN;
   agg.path = (plain || full ? 0 : PMCMC_PATH_FUSED_SWEEP) |
              (tp.coop && !plain && !full ? PMCMC_PATH_COOPERATIVE : 0) |
              (!plain && !logistic && !persist && !h->force_eager && !h->profiling
                   ? PMCMC_PATH_GRAPH
                   : 0) |
              (persist ? PMCMC_PATH_PERSISTENT : 0) |
-             (use_tc ? PMCMC_PATH_TENSOR_CORE : 0) | (full ? PMCMC_PATH_FULL_JACOBIAN : 0);
+             (use_tc ? PMCMC_PATH_TENSOR_CORE : 0) | (full ? PMCMC_PATH_FULL_JACOBIAN : 0) |
+             (logistic && !plain && !f64 ? PMCMC_PATH_TIE_FP64 : 0);
   if (info) *info = agg;
   return status_error(h, status);
 }

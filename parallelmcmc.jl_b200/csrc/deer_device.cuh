@@ -58,6 +58,9 @@ struct DevParams {
   double* lpy;
   uint8_t* acc_col;
   double* la_col;
+  // log alpha of every column with near-tie columns recomputed in FP64
+  // (logistic_tie.cu); nullptr: the sweep forms log alpha itself
+  const double* la_ref;
   double tau;  // prior precision
   // tape of the block, written once by the init kernel: xi (T x Dp, FP32,
   // padded rows zero) and log(u_t) in FP64

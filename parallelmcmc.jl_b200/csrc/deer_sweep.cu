@@ -81,6 +81,8 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
     }
   }
   la = warp_sum(la) + (P.lpy[t] - P.lpx[t]);
+  // near-tie columns: the FP64 value of the same log alpha (logistic_tie.cu)
+  if (P.la_ref) la = P.la_ref[t];
   const double logu = P.logu[t];
   const bool acc = logu < la;
   const Real gp = sigmoid_slope<Real>(la - logu);
@@ -637,7 +639,9 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // Logistic finalize: copy the kept columns out, logp(S_t) from the likelihood
 // sums of the last logp pass (left in lpx) plus the prior, and the accept
-// flags / margins recorded by the last sweep.
+// flags / margins of acc_col / la_col: those of the verification pass at the
+// returned trajectory (fused path), or of the last sweep (plain path, whose
+// max_defect the host reports as NaN).
 // ---------------------------------------------------------------------------
 template <typename Real>
 __global__ void __launch_bounds__(kThreads)
@@ -685,7 +689,6 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (r_acc[0]) atomicAdd(&st->n_accept, r_acc[0]);
     atomicMin(&st->min_margin_bits, dbits(r_mm[0]));
-    if (blockIdx.x == 0) atomicMax(&st->max_defect_bits, 0x7ff8000000000000ull);
   }
 }
 

@@ -46,4 +46,31 @@ int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T);
 // when it gave up.
 cudaError_t lg_tc_mbar_bound(cudaStream_t s, int* err);
 
+// Near-tie decisions in FP64 and the verification pass (logistic_tie.cu).
+// Scratch of one refinement over at most kmax columns.
+struct TieBufs {
+  int kmax = 0;
+  float* mg = nullptr;      // [T] |log alpha - log u| of the sweep
+  int32_t* list = nullptr;  // [kmax] selected columns, ascending
+  int32_t* info = nullptr;  // [4] selected, inside the widest band, band index
+  double *Bx = nullptr, *By = nullptr, *GX = nullptr, *G = nullptr, *G2 = nullptr;  // [kmax x Dp]
+  double* L = nullptr;                                                            // [kmax x N]
+  double *lpx = nullptr, *lpy = nullptr;                                          // [kmax]
+};
+size_t lg_tie_ws_bytes(const LogisticDev& X, int64_t T, int kmax);
+TieBufs lg_tie_carve(void* ws, const LogisticDev& X, int64_t T, int kmax);
+// log alpha of every column as the sweep forms it -> la_ref, |margin| -> mg.
+cudaError_t lg_margin(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS,
+                      int64_t T, double* la_ref, float* mg);
+// lg_margin, then FP64 log alpha for the columns whose margin is below `band`
+// (or a quarter, sixteenth, sixty-fourth of it, the widest that fits kmax),
+// written over their la_ref entries.  cb must be on stream s.
+int lg_tie_refine(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
+                  const DevParams* dP, const DevState* dS, int64_t T, double* la_ref,
+                  const TieBufs& b, float band);
+// Accept flags, margins and the recursion defect at the returned trajectory from
+// la_ref and the passes' proposals (into acc_col, la_col, max_defect_bits).
+cudaError_t lg_verify(cudaStream_t s, bool f64, const DevParams* dP, DevState* dS, int64_t T,
+                      const double* la_ref);
+
 }  // namespace pmcmc

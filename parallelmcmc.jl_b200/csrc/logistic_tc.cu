@@ -8,8 +8,12 @@
 //          s = p (1 - p) L_tangent, loglik = y_n L - softplus(L)  (bayes_logreg.jl:118-154)
 //   GEMM2  G[d, t] += sum_n X[n, d] R[n, t],  R = [r | s]       (M = 128 values of d)
 // The N x 2T intermediate never leaves the SM: L lives in TMEM, R in shared
-// memory, G accumulates in TMEM across all row blocks.  The same shared-memory
-// X tile is GEMM1's K-major A operand and GEMM2's MN-major A operand.
+// memory.  G starts afresh in TMEM at every 128-row block and the epilogue
+// threads add the blocks' partial sums in registers (round-to-nearest FP32):
+// one TMEM accumulation chain over all N rows left the N = 10000 gradient about
+// 10x less accurate than an FP32 SGEMM, enough to move the chain by 1.5e-5.
+// The same shared-memory X tile is GEMM1's K-major A operand and GEMM2's
+// MN-major A operand.
 //
 // Precision: X, the value columns and r are carried as FP16 hi + lo pairs
 // (about 22 significant bits); each value-column product is
@@ -362,7 +366,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
               const uint64_t ah = sdesc(su32(sXh + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
               const uint64_t al = sdesc(su32(sXl + 2 * h * kBoxX) + kn * 2048, kBoxX, 1024, 2);
               const uint64_t br = sdesc(su32(sR) + kn * 2048, kRAtom, 1024, 2);
-              const uint32_t acc = (nb > 0 || kn > 0) ? 1u : 0u;
+              // every row block starts G afresh: the epilogue has added the
+              // previous block's G into its registers before it wrote R
+              const uint32_t acc = kn > 0 ? 1u : 0u;
               mma_f16(tG + 128 * h, ah, br, i2_all, acc);
               mma_f16(tG + 128 * h, al, br, i2_v, 1);
             }
@@ -400,6 +406,30 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     for (int t = 0; t < BH; ++t) ls[t] = lc[t] = 0.f;
     bool ok = true;
     float y_next = row < N ? __ldg(ylab + row) : 0.f;  // label of this row, one block ahead
+    // G accumulates one row block at a time in TMEM; the blocks' partial sums
+    // are added here, in FP32 with round-to-nearest.  Part 2 h + b owns d-half
+    // h of G, the value block (b = 0, hi*lo columns added) or the tangent block.
+    const bool g_owner = has_g && part < 2 * nh;
+    const int gh = part >> 1, gb = part & 1;
+    float gacc[BT];
+#pragma unroll
+    for (int t = 0; t < BT; ++t) gacc[t] = 0.f;
+    auto add_g = [&]() {
+      const uint32_t ga = tG + 128 * gh + lane_off + BT * gb;
+#pragma unroll
+      for (int c = 0; c < BT; c += 8) {
+        float a[8], b8[8], unused[8];
+        if (gb == 0) {
+          tmem_ld8x3(ga + c, tG + 128 * gh + lane_off + 2 * BT + c, ga + c, a, b8, unused);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) gacc[c + i] += a[i] + b8[i];
+        } else {
+          tmem_ld8x3(ga + c, ga + c, ga + c, a, b8, unused);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) gacc[c + i] += a[i];
+        }
+      }
+    };
     for (int nb = 0; nb < nblocks; ++nb) {
       const int64_t n = static_cast<int64_t>(nb) * BN + row;
       const bool valid = n < N;
@@ -407,6 +437,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
+      // GEMM2 of the previous block ran before this block's GEMM1 completed
+      if (g_owner && nb > 0) add_g();
       float v[BH], vl[BH], w[BH];
       tmem_ld8x3(tL + lane_off + BH * part, tL + lane_off + 2 * BT + BH * part,
                  tL + lane_off + BT + BH * part, v, vl, w);
@@ -449,23 +481,14 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     }
     if (ok && has_g && mbar_wait(bar_g + (nh - 1), (nblocks - 1) & 1, err)) {
       tc_fence_after();
-      // part 2 h + b reads d-half h of G, the value block (b = 0) or the tangent block
-      if (part < 2 * nh) {
-        const int h = part >> 1, b = part & 1;
-        float g[32];
-        tmem_ld32(tG + 128 * h + lane_off + BT * b, g);
-        if (b == 0) {  // value columns: add the hi*lo part
-          float gl[32];
-          tmem_ld32(tG + 128 * h + lane_off + 2 * BT, gl);
-#pragma unroll
-          for (int t = 0; t < BT; ++t) g[t] += gl[t];
-        }
-        const int64_t d = 128 * h + row;
+      if (g_owner) {
+        add_g();  // the last row block
+        const int64_t d = 128 * gh + row;
         if (d < Dp) {
-          const int64_t cbase = b ? T : 0;
+          const int64_t cbase = gb ? T : 0;
 #pragma unroll
           for (int t = 0; t < BT; ++t)
-            if (t0 + t < T) G[(cbase + t0 + t) * Dp + d] = g[t];
+            if (t0 + t < T) G[(cbase + t0 + t) * Dp + d] = gacc[t];
         }
       }
     } else if (!ok) {
@@ -702,7 +725,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
           const uint64_t ah = sdesc(su32(sXh + 2 * p * kBoxX) + kn * 2048, kBoxX, 1024, 2);
           const uint64_t al = sdesc(su32(sXl + 2 * p * kBoxX) + kn * 2048, kBoxX, 1024, 2);
           const uint64_t br = sdesc(su32(sR) + kn * 2048, kRAtom, 1024, 2);
-          const uint32_t acc = (nb > 0 || kn > 0) ? 1u : 0u;
+          // every row block starts G afresh (the epilogue adds the blocks up)
+          const uint32_t acc = kn > 0 ? 1u : 0u;
           mma_f16(tG(q), ah, br, i2_all, acc);
           mma_f16(tG(q), al, br, i2_v, 1);
         }
@@ -782,6 +806,21 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     for (int t = 0; t < BH; ++t) ls[t] = lc[t] = 0.f;
     bool ok = true;
     float y_next = row < N ? __ldg(ylab + row) : 0.f;
+    // part q owns d quarter q of G: the row blocks' partial sums of its value
+    // (hi*lo added) and tangent columns, added in FP32 with round-to-nearest
+    float gv[BTW], gt[BTW];
+#pragma unroll
+    for (int t = 0; t < BTW; ++t) gv[t] = gt[t] = 0.f;
+    auto add_g = [&]() {
+      float a[16], b[16], c[16], unused[16];
+      tmem_ld16x2(tG(part) + lane_off, tG(part) + lane_off + 2 * BTW, a, b);
+      tmem_ld16x2(tG(part) + lane_off + BTW, tG(part) + lane_off + BTW, c, unused);
+#pragma unroll
+      for (int t = 0; t < BTW; ++t) {
+        gv[t] += a[t] + b[t];
+        gt[t] += c[t];
+      }
+    };
     for (int nb = 0; nb < nblocks; ++nb) {
       const int64_t n = static_cast<int64_t>(nb) * BN + row;
       const bool valid = n < N;
@@ -789,6 +828,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
+      // GEMM2 of the previous block ran before this block's GEMM1 completed
+      if (has_g && nb > 0) add_g();
       float v[BH], vl[BH], w[BH];
       tmem_ld4x3(tL + lane_off + BH * part, tL + lane_off + 2 * BTW + BH * part,
                  tL + lane_off + BTW + BH * part, v, vl, w);
@@ -830,17 +871,13 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
     }
     if (ok && has_g && mbar_wait(bar_g, (nblocks - 1) & 1, err)) {
       tc_fence_after();
-      // part q reads d quarter q of G: value (+ its hi*lo part) and tangent
-      const int q = part;
-      float g[16], gl[16], gt[16], unused[16];
-      tmem_ld16x2(tG(q) + lane_off, tG(q) + lane_off + 2 * BTW, g, gl);
-      tmem_ld16x2(tG(q) + lane_off + BTW, tG(q) + lane_off + BTW, gt, unused);
-      const int64_t d = 128 * q + row;
+      add_g();  // the last row block
+      const int64_t d = 128 * part + row;
       if (d < Dp) {
 #pragma unroll
         for (int t = 0; t < BTW; ++t)
           if (t0 + t < T) {
-            G[(t0 + t) * Dp + d] = g[t] + gl[t];
+            G[(t0 + t) * Dp + d] = gv[t];
             G[(T + t0 + t) * Dp + d] = gt[t];
           }
       }

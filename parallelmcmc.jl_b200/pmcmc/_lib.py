@@ -87,7 +87,7 @@ class FleetChain(C.Structure):
 
 
 PATH_BITS = [(1, "fused_sweep"), (2, "cooperative"), (4, "graph"), (8, "tensor_core"),
-             (16, "full_jacobian"), (32, "persistent")]
+             (16, "full_jacobian"), (32, "persistent"), (64, "tie_fp64")]
 
 
 _vp = C.c_void_p
