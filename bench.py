@@ -3,29 +3,39 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step" = one DEER block solved to convergence, tape generation
-and per-sample logp included): the anisotropic diagonal Gaussian, D = 100,
-precisions log-uniform in [1e-2, 1e2] (seed 1), eps = 0.05, T = 16384,
-jacobian = :diag, FP32 state, x0 ~ N(0, I), sampler defaults otherwise.
-The path does not shard (one chain), so N GPUs run N independent replicas
-(different tape seeds): weak scaling, no data-path collective.
+Headline workload (the metric's batched + mixed-precision configuration):
+Bayesian logistic regression, N = 10000 rows, D = 256, X iid N(0,1)/sqrt(D),
+theta* ~ N(0, I), y ~ Bernoulli(sigmoid(X theta*)), prior N(0, I), all from
+seed 2; eps = 0.01, T = 65536, :stoch_diag with one probe, FP32 state.  One
+step is one block of T samples solved to convergence: tape generation, every
+Newton sweep (two tensor-core contraction passes, the FP64 decisions of
+near-tie columns, the fused finish + scan), the verification pass at the
+returned trajectory and the per-sample logp.  The stopping rule is
+1e-7 + 1e-6 max|S|: the sampler's default (1e-6 + 1e-5 max|S|) bounds the last
+step, and leaves the iterate about 1.2e-5 from the fixed point, above the
+metric's 1e-5 trace-error bar.  A block that stops unconverged or non-finite
+fails the run.  The path does not shard (one chain), so N GPUs run N
+independent replicas (different tape seeds): weak scaling, no collective on
+the data path.
 
-Printed JSON: value = device-timed samples/s with inputs resident in HBM (L2
-flushed between steps), e2e = the same through pmcmc.sample() with host
-buffers (one call of 8 blocks per step, wall clock; e2e.one_block: one block
-per call), plain_gpu = the unfused reference-structured GPU path, roofline of
-the sweep kernel, cpu_baseline = the FP64 CPU restatement of the reference
-algorithm on this host's cores.
+Printed JSON: value = device-timed samples/s with the data resident in HBM
+(L2 flushed between steps); e2e = the same through pmcmc.sample() with host
+buffers; plain_gpu = the reference-structured GPU path (unfused kernels, cuBLAS
+FP32 contractions, host convergence test) on the same blocks; parity = a timed
+block against the FP64 sequential chain; roofline of the tensor-core pass;
+cpu_baseline = the FP64 restatement of the reference's CPU DEER on this host.
 
-Secondary measurements (not the headline line; 1 GPU):
-    python bench.py --workload logistic_n10k_d256    # N=10000, D=256, T=65536, :stoch_diag
+Secondary measurements (1 GPU):
+    python bench.py --workload aniso_diag_d100       # D=100, T=16384, :diag (persistent kernel)
     python bench.py --workload corr_gauss_d64_full   # D=64, T=8192, :full
     python bench.py --workload logistic_fleet        # 32 uneven logistic chains (N, T / 4)
+    python bench.py --workload logistic_n10k_d256 --dim 512   # the wide tensor-core pass
 --small shrinks T (logistic 4096, correlated Gaussian 1024) for profiler captures.
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -37,20 +47,36 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "parallelmcmc.jl_b200"))
 
 METRIC = "DEER samples/sec, batched+mixed vs plain GPU DEER, at trace err ≤1e-5 vs FP64"
-WORKLOAD = "diag_gauss_D100_T16384_diag_f32"
-E2E_BLOCKS = 8  # blocks of T samples per end-to-end sample() call
-STEP_BLOCKS = 8  # blocks of T samples per timed device-resident sample() call
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes per launch of the profiled kernels, from ncu captures (kernel, workload, bytes)
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "dram_traffic.txt")
 L2_FLUSH_BYTES = 512 << 20
+TOL = (1e-7, 1e-6)   # headline stopping rule (tol_abs, tol_rel)
+REF_T = 128          # reference arm: columns of each complete CPU solve
+CPU_T = 256          # cpu_baseline of our arm: columns of the CPU solve
 
 
 def peaks():
     try:
         with open(PEAKS_PATH) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return p, "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+def traffic_of(kernel: str, workload: str):
+    """DRAM bytes a launch of `kernel` on `workload` moved in an ncu capture, or None."""
+    try:
+        with open(TRAFFIC_PATH) as f:
+            for ln in f:
+                p = ln.split()
+                if len(p) >= 3 and not ln.startswith("#") and p[0] == kernel and p[1] == workload:
+                    return int(p[2])
+    except OSError:
+        pass
+    return None
 
 
 class ClockSampler:
@@ -113,72 +139,96 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_reference_block(model, sampler, x0, seed, block, nthreads):
-    """The FP64 CPU restatement of the reference algorithm (per-t :diag with D JVPs
-    per column, DEER.jl:420-468; Hillis-Steele scan, DEERScan.jl:102-173) on one block."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-    import oracle as O
-    tg = model.target
-    otg = O.Target.diag_gauss(tg["prec"], tg["mean"])
-    Xi, u = O.tape(seed, block, model.dim, sampler.T)
-    t0 = time.perf_counter()
-    S, info = O.deer_solve(otg, sampler.epsilon, np.asarray(x0, np.float64), Xi, u, seed, block,
-                           jacobian=sampler.jacobian, damping=sampler.damping,
-                           tol_abs=sampler.tol_abs, tol_rel=sampler.tol_rel,
-                           maxiter=sampler.maxiter, probes=sampler.probes, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    return S, info, dt
+def headline(T=65536):
+    from pmcmc import configs
+    model, sampler, x0, meta = configs.logistic_n10k_d256(T=T)
+    sampler = dataclasses.replace(sampler, tol_abs=TOL[0], tol_rel=TOL[1])
+    return model, sampler, x0, meta
 
 
-def cpu_sequential_block(model, sampler, x0, seed, block):
-    """The sequential taped MALA chain (MALA.jl:322-346, 377-411) on one block, one
-    thread, FP64: the trace DEER reproduces."""
+def workload_name(T=65536):
+    return f"logistic_N10000_D256_T{T}_stoch_diag_f32"
+
+
+def trace_err(S, R):
+    import numpy as np
+    return float(np.max(np.linalg.norm(S - R, axis=0) /
+                        np.maximum(np.linalg.norm(R, axis=0), 1e-30)))
+
+
+# --------------------------------------------------------------------------- CPU legs
+def cpu_deer_solve(model, sampler, seed, block, T):
+    """One complete solve of a T-column block by the FP64 NumPy restatement of the
+    reference's CPU DEER on the batched :stoch_diag branch (twelve BLAS GEMMs a
+    sweep, MALA.jl:556-628 with bayes_logreg.jl:91-206; doubling scan,
+    DEERScan.jl:102-173), BLAS on every host thread."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
+    import np_oracle as NP
     import oracle as O
     tg = model.target
-    otg = O.Target.diag_gauss(tg["prec"], tg["mean"])
-    Xi, u = O.tape(seed, block, model.dim, sampler.T)
+    D = model.dim
+    m = NP.logistic_batched_model(tg["X"], tg["y"], tg["prior_prec"])
+    Xi, u = O.tape(seed, block, D, T)
     t0 = time.perf_counter()
-    O.mala_sequential(otg, sampler.epsilon, np.asarray(x0, np.float64), Xi, u)
-    return time.perf_counter() - t0
+    _, info = NP.deer_solve_batched(m, sampler.epsilon, np.zeros(D), np.asarray(Xi, np.float64),
+                                    u, lambda it: O.probe(seed, block, it, 0, D, T),
+                                    tol_abs=sampler.tol_abs, tol_rel=sampler.tol_rel,
+                                    maxiter=sampler.maxiter, damping=sampler.damping)
+    return info, time.perf_counter() - t0
+
+
+def blas_threads():
+    try:
+        import threadpoolctl
+        return max(i.get("num_threads", 1) for i in threadpoolctl.threadpool_info()
+                   if i.get("user_api") == "blas")
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return
-    from pmcmc import configs
-    model, sampler, x0, meta = configs.aniso_diag_d100()
-    nthreads = os.cpu_count() or 1
+    model, sampler, x0, meta = headline()
     for w in range(args.warmup):
-        cpu_reference_block(model, sampler, x0, meta["seed"], w, nthreads)
+        cpu_deer_solve(model, sampler, meta["seed"], w, REF_T)
     times, iters = [], []
     for k in range(args.steps):
-        _, info, dt = cpu_reference_block(model, sampler, x0, meta["seed"], args.warmup + k,
-                                          nthreads)
+        info, dt = cpu_deer_solve(model, sampler, meta["seed"], args.warmup + k, REF_T)
+        if not info["converged"]:
+            raise SystemExit(f"reference CPU DEER: block {args.warmup + k} not converged: {info}")
         times.append(dt)
         iters.append(info["iters"])
     total = sum(times)
-    value = args.steps * sampler.T / total
+    value = args.steps * REF_T / total
+    nth = blas_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, see config)",
-        "config": {"workload": WORKLOAD, "D": 100, "T": sampler.T, "eps": 0.05,
-                   "jacobian": "diag", "newton_iters_mean": statistics.mean(iters)},
-        "cpu_baseline": {"value": value, "unit": "samples/s", "cores": nthreads, "kind": "port",
-                         "sample": "full blocks: FP64 C restatement of the reference CPU DEER "
-                                   "(per-t :diag with D JVPs per column, doubling scan), OpenMP"},
+        "config": {"workload": workload_name(), "N": 10000, "D": 256, "T": 65536, "eps": 0.01,
+                   "jacobian": "stoch_diag", "tol_abs": TOL[0], "tol_rel": TOL[1],
+                   "sample": f"each step one complete solve of a {REF_T}-column block of this "
+                             f"target (a 65536-column block takes about 55 sweeps of ~2 min "
+                             f"each on the CPU; sweeps a solve grow with T, so this rate is "
+                             f"an upper bound for full blocks)",
+                   "newton_iters_mean": statistics.mean(iters)},
+        "cpu_baseline": {"value": value, "unit": "samples/s", "cores": nth, "kind": "port",
+                         "sample": f"complete {REF_T}-column solves: FP64 NumPy restatement of "
+                                   f"the reference's batched CPU DEER (12 BLAS GEMMs a sweep, "
+                                   f"single-threaded elementwise work as Julia broadcasts)"},
         "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "Julia is not installed; the reference arm is the oracle port of its algorithm",
+        "note": "Julia is not installed on the GPU box; the reference arm is the oracle port "
+                "of its algorithm",
     }
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- our arm
 def run_ours(args):
     import ctypes as C
 
@@ -187,7 +237,6 @@ def run_ours(args):
 
     import pmcmc
     from pmcmc import _lib as L
-    from pmcmc import configs
 
     world, rank, local = dist_setup()
     pg = None
@@ -199,19 +248,17 @@ def run_ours(args):
         pg = dist
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    # one explicit stream for the L2 flush, the CUDA events and the library, so that
-    # the events bracket the solve (torch's default stream is the legacy stream 0,
-    # which a handle would replace by a non-blocking stream of its own)
+    # one explicit stream for the L2 flush, the CUDA events and the library
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     h = pmcmc.Handle(local, stream=stream.cuda_stream)
     lib = L.load()
 
-    model, sampler, x0, meta = configs.aniso_diag_d100()
-    D, T = model.dim, sampler.T
+    model, sampler, x0, meta = headline()
+    D, T, N = model.dim, sampler.T, model.target["X"].shape[0]
     seed = meta["seed"] + 7919 * rank  # replicas: each rank its own tape stream
     tgt = model.device_target(h)
-    x0_dev = torch.from_numpy(np.asarray(x0)).to(dev)
+    x0_dev = torch.from_numpy(np.asarray(x0, np.float32)).to(dev)
     S_dev = torch.empty((T, D), dtype=torch.float32, device=dev)
     lp_dev = torch.empty((T,), dtype=torch.float32, device=dev)
     acc_dev = torch.empty((T,), dtype=torch.uint8, device=dev)
@@ -226,235 +273,273 @@ def run_ours(args):
         L.check(rc, h.ptr, "deer_solve")
         return info
 
-    def timed(smp, nsteps, block0):
+    def timed(smp, blocks):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(nsteps)]
+              for _ in blocks]
         infos = []
-        for k in range(nsteps):
+        for k, b in enumerate(blocks):
             flush.zero_()  # L2 flush (512 MB > 126 MB L2), outside the timed events
             ev[k][0].record(stream)
-            infos.append(solve_dev(smp, block0 + k))
+            infos.append(solve_dev(smp, b))
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
         return [a.elapsed_time(b) for a, b in ev], infos
 
-    # A step is one sample() call of STEP_BLOCKS blocks into HBM buffers: block b + 1
-    # starts from block b's last column on the device, the blocks run back to back.
-    S_run = torch.empty((STEP_BLOCKS * T, D), dtype=torch.float32, device=dev)
-    lp_run = torch.empty((STEP_BLOCKS * T,), dtype=torch.float32, device=dev)
-    acc_run = torch.empty((STEP_BLOCKS * T,), dtype=torch.uint8, device=dev)
+    def check_converged(infos, blocks, what):
+        for b, i in zip(blocks, infos):
+            if not i.converged or i.status:
+                line = {"metric": METRIC, "value": None, "unit": "samples/s",
+                        "error": f"{what}: block {b} not converged (iters {i.iters}, metric "
+                                 f"{i.metric:.3g}, status {i.status}); unconverged blocks are "
+                                 f"not samples"}
+                print(json.dumps(line), flush=True)
+                raise SystemExit(1)
 
-    def timed_run(smp, nsteps, seed0):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(nsteps)]
-        infos = []
-        for k in range(nsteps):
-            flush.zero_()
-            ev[k][0].record(stream)
-            info = L.Info()
-            p = smp.params()
-            rc = lib.pmcmc_sample(h.ptr, tgt, C.byref(p), x0_dev.data_ptr(), seed0 + k,
-                                  STEP_BLOCKS * T, S_run.data_ptr(), lp_run.data_ptr(),
-                                  acc_run.data_ptr(), L.MEM_DEVICE, C.byref(info))
-            L.check(rc, h.ptr, "sample")
-            ev[k][1].record(stream)
-            infos.append(info)
-        torch.cuda.synchronize(dev)
-        return [a.elapsed_time(b) for a, b in ev], infos
-
-    # ---- warm-up and timed region (device-resident inputs/outputs)
-    timed_run(sampler, args.warmup, seed + 100)
+    # ---- warm-up and timed region (data and outputs in HBM)
+    timed(sampler, [100 + w for w in range(args.warmup)])
+    blocks = [1000 + k for k in range(args.steps)]
     if pg:
         pg.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        ms, infos = timed_run(sampler, args.steps, seed + 1000)
+        ms, infos = timed(sampler, blocks)
     torch.cuda.synchronize(dev)
+    check_converged(infos, blocks, "timed")
     total_ms = sum(ms)
     if pg:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * args.steps * STEP_BLOCKS * T / (total_ms / 1e3)
-    iters = [i.iters / STEP_BLOCKS for i in infos]  # Newton sweeps a block
-    persistent = bool(infos[0].path & 32)
-    # one cooperative launch per block (persistent solve), else init + sweeps + finalize
-    launches = sum(STEP_BLOCKS * (1 if persistent else 2) + (0 if persistent else i.iters)
-                   for i in infos)
-    # the same blocks one solve() call each (a host round trip between blocks)
-    timed(sampler, 2, 0)
-    ms1, _ = timed(sampler, args.steps, 1000)
-    value_one_call = world * args.steps * T / (sum(ms1) / 1e3)
+    value = world * args.steps * T / (total_ms / 1e3)
+    iters = [i.iters for i in infos]
+    # kernels of ours a block: init; a sweep = 2 passes x (operand split, tensor-core
+    # pass, mid) + near-tie selection (margin, select, gather, 2 x loglik, propose,
+    # final) + the finish-and-scan sweep kernel; the verification the same without the
+    # sweep kernel plus the verify kernel; the logp pass (split, tensor-core pass);
+    # finalize.  cuBLAS DGEMMs of the near-tie columns are not counted.
+    per_sweep = 6 + 7 + 1
+    launches = sum(1 + per_sweep * i.iters + (6 + 7 + 1) + 2 + 1 for i in infos)
 
-    # ---- parity of the timed workload: first timed block vs the FP64 sequential oracle
-    parity = {}
-    if rank == 0:
-        try:
-            sys.path.insert(0, os.path.join(ROOT, "oracle"))
-            import oracle as O
-            solve_dev(sampler, 1000)
-            S = S_dev.cpu().numpy().T.astype(np.float64)
-            acc = acc_dev.cpu().numpy().astype(bool)
-            Xi, u = O.tape(seed, 1000, D, T)
-            otg = O.Target.diag_gauss(model.target["prec"])
-            S_seq, acc_seq, _ = O.mala_sequential(otg, sampler.epsilon,
-                                                  np.asarray(x0, np.float64), Xi, u)
-            err = float(np.max(np.linalg.norm(S - S_seq, axis=0) /
-                               np.maximum(np.linalg.norm(S_seq, axis=0), 1e-30)))
-            parity = {"trace_err_vs_fp64": err, "accept_identical": bool(np.array_equal(acc, acc_seq)),
-                      "accept_rate": float(acc.mean())}
-        except Exception as e:  # parity is reported, never fatal for the timing
-            parity = {"error": repr(e)}
-
-    # ---- plain GPU DEER (unfused, reference-structured) on the same workload
-    plain = pmcmc.ParallelMALASampler(sampler.epsilon, T=T, jacobian=sampler.jacobian,
-                                      dtype=np.float32, exec="plain")
-    timed_run(plain, 1, seed + 1900)
-    pms, pinfos = timed_run(plain, max(3, args.steps // 4), seed + 2000)
-    plain_value = len(pms) * STEP_BLOCKS * T / (sum(pms) / 1e3)
-
-    # ---- roofline of the dominant kernel (the fused sweep), CUDA events per launch
-    h.set_profiling(True)
-    for k in range(max(3, args.steps // 2)):
-        flush.zero_()
-        solve_dev(sampler, 3000 + k)
-    torch.cuda.synchronize(dev)
-    prof = h.profile(reset=True)
-    h.set_profiling(False)
-    sweep_bytes = 12 * D * T + 8 * T  # one Newton sweep (S read, Xi read, S write, u read, logp write)
-    hbm, src = peaks()
-    if prof["solve_launches"]:
-        # persistent kernel: one launch = tape + every sweep + verification of a block
-        kernel = "deer_persist_kernel"
-        launch_ms = prof["solve_ms"] / prof["solve_launches"]
-        sweeps = prof["solve_sweeps"] / prof["solve_launches"]
-        alg_bytes = sweeps * sweep_bytes
-        min_bytes = 4 * D * T + 5 * T  # S, logp, accept out; S and the tape stay on chip
-        nprof = prof["solve_launches"]
-        # dram__bytes_read.sum + dram__bytes_write.sum per block, from the ncu capture of
-        # an 8-block launch of this workload (136,704 + 1,610,240 B over 8 blocks),
-        # summarised in profiles/deer_persist_kernel_aniso_diag_d100.md
-        traffic = 218368
-    else:
-        kernel = "deer_sweep_kernel"
-        launch_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
-        sweeps = 1.0
-        alg_bytes = sweep_bytes
-        min_bytes = 8 * D * T + 4 * T  # what this kernel must move (tape regenerated in registers)
-        nprof = prof["sweep_launches"]
-        # dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of this workload,
-        # from the ncu capture summarised in profiles/deer_sweep_kernel_aniso_diag_d100.md
-        traffic = 6754048
-    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
-
-    # ---- sequential MALA on the device (pmcmc_mala_chains): one chain over the same
-    # block, and a chain a warp on every SM for throughput
-    def chains_rate(n):
-        x0c = x0_dev.repeat(n, 1).contiguous()
-        sd = torch.arange(n, dtype=torch.int64, device=dev) + seed
-        Sc = torch.empty((n, T, D), dtype=torch.float32, device=dev)
-        p = sampler.params()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        L.check(lib.pmcmc_mala_chains(h.ptr, tgt, C.byref(p), n, x0c.data_ptr(), sd.data_ptr(),
-                                      1000, Sc.data_ptr(), None, None, L.MEM_DEVICE), h.ptr,
-                "mala_chains")
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        return n * T / (e0.elapsed_time(e1) / 1e3)
-
-    chains_rate(1)
-    seq_one = chains_rate(1)
-    seq_many = chains_rate(8 * torch.cuda.get_device_properties(dev).multi_processor_count)
-
-    # ---- end to end through the public API with host buffers: one sample() call of
-    # E2E_BLOCKS blocks per step (x0 in, the chain's values, logp and accept flags out;
-    # block b's copy-out overlaps block b + 1's solve), and of one block for reference
+    # ---- end to end through the public API with host buffers: pmcmc.sample of one
+    # block per step (x0 from pinned memory in, the chain's values, logp and accept
+    # flags out to host memory), wall clock
     x0_host = torch.tensor(np.asarray(x0, np.float32)).pin_memory().numpy()
 
-    def e2e(nblocks, nsteps):
-        pmcmc.sample(model, sampler, nblocks * T, seed=seed, initial_params=x0_host, handle=h)
-        ts = []
+    def e2e(nsteps):
+        pmcmc.sample(model, sampler, T, seed=seed + 1, initial_params=x0_host, handle=h)
+        ts, oks = [], True
         for k in range(nsteps):
             t0 = time.perf_counter()
-            pmcmc.sample(model, sampler, nblocks * T, seed=seed + 1 + k, initial_params=x0_host,
-                         handle=h)
+            ch = pmcmc.sample(model, sampler, T, seed=seed + 2 + k, initial_params=x0_host,
+                              handle=h)
             ts.append(time.perf_counter() - t0)
+            oks &= bool(ch.info["converged"])
         total = sum(ts)
         if pg:
             t = torch.tensor([total], device=dev, dtype=torch.float64)
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             total = float(t.item())
-        return world * nsteps * nblocks * T / total
+        return world * nsteps * T / total, oks
 
-    e2e_val = e2e(E2E_BLOCKS, max(3, args.steps // 2))
-    e2e_one = e2e(1, max(3, args.steps // 2))
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        nthreads = os.cpu_count() or 1
-        _, cinfo, cdt = cpu_reference_block(model, sampler, x0, seed, 0, nthreads)
-        cpu = {"value": T / cdt, "unit": "samples/s", "cores": nthreads, "kind": "port",
-               "sample": f"one full block (T={T}): FP64 C restatement of the reference CPU DEER "
-                         f"(per-t :diag, D JVPs per column, doubling scan), "
-                         f"{cinfo['iters']} Newton iterations, OpenMP"}
-        sdt = cpu_sequential_block(model, sampler, x0, seed, 0)
-        cpu["sequential_mala"] = {"value": T / sdt, "unit": "samples/s", "cores": 1,
-                                  "sample": f"the sequential taped MALA chain over the same "
-                                            f"block (T={T}), FP64 C, one thread"}
-
+    e2e_val, e2e_ok = e2e(max(3, args.steps // 4))
     if pg:
         pg.barrier()
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded NumPy PCG64 + counter-based Philox tape)",
-            "config": {"workload": WORKLOAD, "D": D, "T": T, "eps": 0.05, "jacobian": "diag",
-                       "step": f"pmcmc_sample of {STEP_BLOCKS} blocks (N={STEP_BLOCKS}*T) into "
-                               f"HBM buffers, x0 in HBM; CUDA events on the launching stream",
-                       "one_block_per_call": {"value": value_one_call, "unit": "samples/s",
-                                              "step": "pmcmc_deer_solve of one block"},
-                       "state": "f32", "logalpha": "f64", "l2": "flushed (512 MB write) "
-                       "between timed steps", "parallelism": f"replicas x{world}",
-                       "newton_iters_mean": statistics.mean(iters),
-                       "path": [n for b, n in L.PATH_BITS if infos[0].path & b]},
-            "e2e": {"value": e2e_val, "unit": "samples/s", "h2d_bytes_per_step": 4 * D,
-                    "d2h_bytes_per_step": E2E_BLOCKS * (4 * D * T + 4 * T + T),
-                    "step": f"pmcmc.sample(N={E2E_BLOCKS}*T) from pinned x0 into pinned host "
-                            f"arrays, wall clock",
-                    "one_block": {"value": e2e_one, "step": "pmcmc.sample(N=T)",
-                                  "d2h_bytes_per_step": 4 * D * T + 4 * T + T}},
-            "gpu_sequential_mala": {"one_chain": seq_one,
-                                    "one_chain_speedup_of_deer": value / world / seq_one,
-                                    "chains_8_per_sm": seq_many, "unit": "samples/s",
-                                    "note": "independent taped MALA chains, one warp each "
-                                            "(pmcmc_mala_chains), same block and tape"},
-            "plain_gpu": {"value": plain_value, "unit": "samples/s",
-                          "newton_iters_mean": statistics.mean(i.iters / STEP_BLOCKS for i in pinfos),
-                          "speedup_fused_over_plain": value / world / plain_value},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
-                         "kernel": kernel, "avg_launch_ms": launch_ms,
-                         "sweeps_per_launch": sweeps,
-                         "alg_bytes_per_launch": alg_bytes,
-                         "kernel_min_bytes_per_launch": min_bytes,
-                         "launches_profiled": nprof},
-            "cpu_baseline": cpu,
-            "parity": parity,
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
-    if pg:
         pg.destroy_process_group()
+    if rank != 0:
+        return
+
+    # ---- parity of a timed block: block 1000 solved again (solves repeat bit for bit)
+    # against the FP64 sequential chain on the same tape
+    parity = {}
+    try:
+        if args.no_parity:
+            raise RuntimeError("skipped (--no-parity)")
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        pinfo = solve_dev(sampler, blocks[0])
+        S = S_dev.cpu().numpy().T.astype(np.float64)
+        acc = acc_dev.cpu().numpy().astype(bool)
+        Xi, u = O.tape(seed, blocks[0], D, T)
+        otg = O.Target.logistic(model.target["X"], model.target["y"])
+        t0 = time.perf_counter()
+        S_seq, acc_seq, la_seq = O.mala_sequential_logistic(otg, sampler.epsilon,
+                                                            np.zeros(D), Xi, u)
+        seq_s = time.perf_counter() - t0
+        m_seq = la_seq - np.log(u.astype(np.float64))
+        parity = {"block": blocks[0], "trace_err_vs_fp64": trace_err(S, S_seq),
+                  "accept_identical": bool(np.array_equal(acc, acc_seq)),
+                  "accept_mismatches": int(np.sum(acc != acc_seq)),
+                  "accept_rate": float(acc.mean()), "newton_iters": pinfo.iters,
+                  "min_margin_fp64_chain": float(np.abs(m_seq).min()),
+                  "min_margin_returned": pinfo.min_margin, "max_defect": pinfo.max_defect,
+                  "fp64_chain": f"oracle sequential chain, {os.cpu_count()} threads, "
+                                f"{seq_s:.1f} s"}
+    except Exception as e:  # parity is reported, never fatal for the timing
+        parity = {"error": repr(e)}
+
+    # ---- plain GPU DEER (reference structure: unfused kernels, cuBLAS FP32
+    # contractions in pedantic mode, host convergence test every sweep) on the first
+    # two timed blocks
+    plain = dataclasses.replace(sampler, exec="plain")
+    pblocks = blocks[:2]
+    pms, pinfos = timed(plain, pblocks)
+    p_ok = all(i.converged and not i.status for i in pinfos)
+    plain_value = len(pms) * T / (sum(pms) / 1e3)
+    same = [ms[k] for k in range(len(pblocks))]
+    plain_gpu = {"value": plain_value, "unit": "samples/s", "blocks": pblocks,
+                 "newton_iters": [i.iters for i in pinfos], "converged": p_ok,
+                 "fused_newton_iters_same_blocks": iters[:len(pblocks)],
+                 "speedup_fused_over_plain": (sum(pms) / sum(same)) if p_ok else None,
+                 "note": "both paths converged on these blocks" if p_ok else
+                         "plain path did not converge: no speed-up reported"}
+
+    # ---- roofline of the dominant kernel: the tensor-core contraction pass, timed
+    # with CUDA events around every pass (profiling mode) over one block
+    pk, src = peaks()
+    h.set_profiling(True)
+    flush.zero_()
+    solve_dev(sampler, 3000)
+    torch.cuda.synchronize(dev)
+    prof = h.profile(reset=True)
+    h.set_profiling(False)
+    pass_ms = prof["pass_ms"] / max(1, prof["pass_launches"])
+    flops = 8.0 * N * D * T  # two GEMMs of 2 N D (2T) per contraction pass
+    tpk = float(pk.get("bf16_tflops_sustained", pk["bf16_tflops"]))
+    achieved = flops / (pass_ms / 1e3) / 1e12
+    kname = "logistic_pass_tc_kernel"
+    roofline = {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": tpk,
+                "unit": "TFLOP/s", "frac": achieved / tpk, "traffic": traffic_of(kname, workload_name()),
+                "peak_source": f"{src}: bf16 dense, sustained (the pass runs inside a "
+                               f"seconds-long solve)",
+                "avg_launch_ms": pass_ms, "launches_timed": prof["pass_launches"],
+                "alg_flops_per_launch": flops,
+                "alg_flops_note": "16 N D T a sweep over its two passes (section 8d); value "
+                                  "columns run three products (hi*hi, lo*hi, hi*lo) and "
+                                  "tangents one, so the tensor pipe executes ~2x",
+                "sweep_kernel_ms": prof["sweep_ms"] / max(1, prof["sweep_launches"])}
+
+    # ---- CPU baselines (bounded samples on this host's cores)
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cinfo, cdt = cpu_deer_solve(model, sampler, seed, 0, CPU_T)
+        cpu = {"value": CPU_T / cdt, "unit": "samples/s", "cores": blas_threads(),
+               "kind": "port",
+               "sample": f"one complete solve of a {CPU_T}-column block of this target "
+                         f"({cinfo['iters']} sweeps, {cdt:.1f} s): FP64 NumPy restatement of "
+                         f"the reference's batched CPU DEER, 12 BLAS GEMMs a sweep; full "
+                         f"65536-column blocks need more sweeps, so this rate is an upper bound"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        Ts = 4096
+        Xi, u = O.tape(seed, 0, D, Ts)
+        otg = O.Target.logistic(model.target["X"], model.target["y"])
+        t0 = time.perf_counter()
+        O.mala_sequential_logistic(otg, sampler.epsilon, np.zeros(D), Xi, u)
+        sdt = time.perf_counter() - t0
+        cpu["sequential_mala"] = {"value": Ts / sdt, "unit": "samples/s",
+                                  "cores": os.cpu_count(),
+                                  "sample": f"the sequential FP64 MALA chain over {Ts} steps "
+                                            f"of the same target (oracle C, threaded sums)"}
+
+    secondary = {}
+    if not args.no_secondary:
+        try:
+            secondary["aniso_diag_d100"] = gauss_secondary(h, lib, stream, dev, flush)
+        except Exception as e:
+            secondary["aniso_diag_d100"] = {"error": repr(e)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded NumPy PCG64 data + counter-based Philox tape)",
+        "config": {"workload": workload_name(), "N": N, "D": D, "T": T,
+                   "eps": sampler.epsilon, "jacobian": "stoch_diag", "probes": 1,
+                   "tol_abs": TOL[0], "tol_rel": TOL[1],
+                   "step": "pmcmc_deer_solve of one block, data and outputs in HBM; CUDA "
+                           "events on the launching stream",
+                   "precision": "FP32 state; contractions on tcgen05 tensor cores with FP16 "
+                                "hi/lo split operands (~22 bits) and FP32 accumulation; "
+                                "log alpha and Newton metric in FP64; near-tie columns "
+                                "decided from an FP64 log alpha",
+                   "l2": "flushed (512 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}",
+                   "newton_iters_mean": statistics.mean(iters),
+                   "newton_iters": [min(iters), max(iters)],
+                   "accept_rate": statistics.mean(i.n_accept / T for i in infos),
+                   "path": [n for b, n in L.PATH_BITS if infos[0].path & b]},
+        "e2e": {"value": e2e_val, "unit": "samples/s", "h2d_bytes_per_step": 4 * D,
+                "d2h_bytes_per_step": 4 * D * T + 4 * T + T, "converged": e2e_ok,
+                "step": "pmcmc.sample(N=T) from a pinned x0 into host arrays (values, logp, "
+                        "accept flags), wall clock"},
+        "plain_gpu": plain_gpu,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "parity": parity,
+        "secondary": secondary,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
 
 
+def gauss_secondary(h, lib, stream, dev, flush):
+    """The D = 100 anisotropic diagonal Gaussian (T = 16384, :diag) on the persistent
+    kernel: 8-block sample() calls into HBM, the same on the plain path, and a chain
+    that moves (eps = 0.005, several sweeps a block)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from pmcmc import _lib as L
+    from pmcmc import configs
+    model, sampler, x0, meta = configs.aniso_diag_d100()
+    D, T, nb = model.dim, sampler.T, 8
+    tgt = model.device_target(h)
+    x0_dev = torch.from_numpy(np.asarray(x0)).to(dev)
+    S = torch.empty((nb * T, D), dtype=torch.float32, device=dev)
+    lp = torch.empty((nb * T,), dtype=torch.float32, device=dev)
+    acc = torch.empty((nb * T,), dtype=torch.uint8, device=dev)
+
+    def run(smp, seeds):
+        out = []
+        for s in seeds:
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = L.Info()
+            p = smp.params()
+            L.check(lib.pmcmc_sample(h.ptr, tgt, C.byref(p), x0_dev.data_ptr(), s, nb * T,
+                                     S.data_ptr(), lp.data_ptr(), acc.data_ptr(), L.MEM_DEVICE,
+                                     C.byref(info)), h.ptr, "sample")
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            out.append((e0.elapsed_time(e1), info))
+        return out
+
+    res = {}
+    for name, smp in (("default", sampler),
+                      ("moving_eps0.005", dataclasses.replace(sampler, epsilon=0.005)),
+                      ("plain", dataclasses.replace(sampler, exec="plain"))):
+        run(smp, [meta["seed"] + 100 + i for i in range(2)])
+        r = run(smp, [meta["seed"] + 1000 + i for i in range(5)])
+        tot = sum(m for m, _ in r)
+        res[name] = {"value": 5 * nb * T / (tot / 1e3), "unit": "samples/s",
+                     "sweeps_per_block": statistics.mean(i.iters / nb for _, i in r),
+                     "accept_rate": statistics.mean(i.n_accept / (nb * T) for _, i in r),
+                     "converged": all(i.converged for _, i in r),
+                     "us_per_block": 1e3 * tot / (5 * nb)}
+    res["workload"] = meta["workload"]
+    res["step"] = f"pmcmc_sample of {nb} blocks into HBM (one persistent launch on the fused path)"
+    return res
+
+
+# --------------------------------------------------------------------------- secondary workloads
 def run_secondary(args):
-    """Logistic regression (tensor-core contraction passes) or the correlated
-    Gaussian in :full mode: device-timed solves, Newton iterations, accept
-    rate, and the roofline of the dominant kernel."""
+    """Logistic regression at another D or T, or the correlated Gaussian in :full
+    mode: device-timed solves, Newton iterations, accept rate, and the roofline of
+    the dominant kernel."""
     import ctypes as C
 
     import numpy as np
@@ -474,6 +559,7 @@ def run_secondary(args):
     if logistic:
         model, sampler, x0, meta = configs.logistic_n10k_d256(T=4096 if args.small else 65536,
                                                               D=args.dim)
+        sampler = dataclasses.replace(sampler, tol_abs=TOL[0], tol_rel=TOL[1])
     else:
         model, sampler, x0, meta = configs.correlated_gauss_d64(T=1024 if args.small else 8192)
         # the sampler's default stopping rule (1e-6 + 1e-5 |S|) allows ~1e-5 relative
@@ -518,7 +604,7 @@ def run_secondary(args):
     torch.cuda.synchronize(dev)
     prof = h.profile(reset=True)
     h.set_profiling(False)
-    hbm, src = peaks()
+    pk, src = peaks()
     line = {"metric": METRIC, "secondary": True, "value": value, "unit": "samples/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": sum(ms) / args.steps, "higher_is_better": True, "dtype": "f32",
@@ -526,39 +612,21 @@ def run_secondary(args):
             "config": {"workload": meta["workload"], "D": D, "T": T, "eps": sampler.epsilon,
                        "jacobian": sampler.jacobian, "tol_abs": sampler.tol_abs,
                        "tol_rel": sampler.tol_rel, "newton_iters_mean": iters,
-                       "accept_rate": acc_rate, "path": infos[-1].as_dict()["path_names"]},
+                       "accept_rate": acc_rate,
+                       "converged": all(i.converged for i in infos),
+                       "path": infos[-1].as_dict()["path_names"]},
             "clocks": clk.summary()}
     if logistic:
-        # plain FP32 GPU DEER on the first timed block: unfused kernels, cuBLAS FP32
-        # contractions, the convergence test on the host after every iteration
-        import dataclasses
-        plain = dataclasses.replace(sampler, exec="plain")
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        flush.zero_()
-        e0.record(stream)
-        pinfo = solve_dev(plain, 1000)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        pms = e0.elapsed_time(e1)
-        line["plain_gpu"] = {"value": T / (pms / 1e3), "unit": "samples/s", "block": 1000,
-                             "newton_iters": pinfo.iters, "converged": bool(pinfo.converged),
-                             "fused_newton_iters_same_block": infos[0].iters,
-                             "speedup_fused_over_plain": value / (T / (pms / 1e3))}
         N = meta.get("N_rows", 10_000)
         pass_ms = prof["pass_ms"] / max(1, prof["pass_launches"])
         flops = 8.0 * N * D * T  # two GEMMs of 2 N D (2T) per contraction pass
-        try:
-            with open(PEAKS_PATH) as f:
-                tpk, tsrc = float(json.load(f)["bf16_tflops"]), "measured (bf16 dense, burst)"
-        except Exception:
-            tpk, tsrc = 1590.0, "fallback"
+        tpk = float(pk.get("bf16_tflops_sustained", pk["bf16_tflops"]))
         achieved = flops / (pass_ms / 1e3) / 1e12
         kname = "logistic_pass_tc_wide_kernel" if D > 256 else "logistic_pass_tc_kernel"
         line["roofline"] = {"bound": "tensor", "kernel": f"{kname} (+ mid kernel)",
                             "achieved": achieved, "peak": tpk, "unit": "TFLOP/s",
-                            "frac": achieved / tpk, "peak_source": tsrc,
+                            "frac": achieved / tpk, "peak_source": f"{src}, sustained",
                             "avg_launch_ms": pass_ms, "alg_flops_per_launch": flops,
-                            "executed_mma_flops_per_launch": 2 * flops,
                             "sweep_ms": prof["sweep_ms"] / max(1, prof["sweep_launches"])}
     else:
         sweep_ms = prof["sweep_ms"] / max(1, prof["sweep_launches"])
@@ -567,6 +635,7 @@ def run_secondary(args):
         # apply: S and S' read and written; log u and accept flags
         alg_bytes = 4 * T * (13 * Dq + 2 * D) + 9 * T
         achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+        hbm = float(pk["hbm_gbs"])
         line["roofline"] = {"bound": "hbm", "kernel": "full sweep (eval+chunk+carry+apply)",
                             "achieved": achieved, "peak": hbm, "unit": "GB/s",
                             "frac": achieved / hbm, "peak_source": src, "avg_sweep_ms": sweep_ms,
@@ -580,10 +649,27 @@ def run_secondary(args):
         Xi, u = O.tape(meta["seed"], 1000, D, T)
         S_seq, acc_seq, _ = O.mala_sequential(O.Target.dense_gauss(model.target["prec"]),
                                               sampler.epsilon, np.asarray(x0, np.float64), Xi, u)
-        line["parity"] = {"trace_err_vs_fp64": float(np.max(
-            np.linalg.norm(S - S_seq, axis=0) / np.maximum(np.linalg.norm(S_seq, axis=0), 1e-30))),
-            "accept_identical": bool(np.array_equal(acc, acc_seq))}
+        line["parity"] = {"trace_err_vs_fp64": trace_err(S, S_seq),
+                          "accept_identical": bool(np.array_equal(acc, acc_seq))}
     print(json.dumps(line), flush=True)
+
+
+def run_gauss(args):
+    """The D = 100 diagonal-Gaussian workload alone (persistent kernel)."""
+    import torch
+
+    import pmcmc
+    from pmcmc import _lib as L
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    h = pmcmc.Handle(0, stream=stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    with ClockSampler(0) as clk:
+        res = gauss_secondary(h, L.load(), stream, dev, flush)
+    res.update({"metric": METRIC, "secondary": True, "clocks": clk.summary()})
+    print(json.dumps(res), flush=True)
 
 
 def run_fleet(args):
@@ -615,9 +701,6 @@ def run_fleet(args):
     pmcmc.fleet_solve(chains, workers=1, handle=h, errors="report")
     torch.cuda.synchronize()
     serial = time.perf_counter() - t0
-    # plain per-chain FP32 GPU DEER (unfused kernels, cuBLAS FP32 contractions, host
-    # convergence test every iteration), the same chains one at a time, one run
-    import dataclasses
     plain_chains = [(m, dataclasses.replace(smp, exec="plain"), *rest)
                     for m, smp, *rest in chains]
     t0 = time.perf_counter()
@@ -664,23 +747,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="aniso_diag_d100",
-                    choices=["aniso_diag_d100", "logistic_n10k_d256", "corr_gauss_d64_full",
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity leg (the FP64 sequential chain on the host)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary diagonal-Gaussian measurements")
+    ap.add_argument("--workload", default="logistic_n10k_d256",
+                    choices=["logistic_n10k_d256", "aniso_diag_d100", "corr_gauss_d64_full",
                              "logistic_fleet"])
     ap.add_argument("--dim", type=int, default=256,
                     help="logistic workload: dimension D (256 < D <= 512 runs the wide "
-                         "tensor-core pass)")
+                         "tensor-core pass); D != 256 or --small is a secondary line")
     ap.add_argument("--small", action="store_true",
                     help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "logistic_fleet" and args.impl == "ours":
-        run_fleet(args)
-    elif args.workload != "aniso_diag_d100" and args.impl == "ours":
-        run_secondary(args)
-    elif args.impl == "reference":
+    if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "logistic_fleet":
+        run_fleet(args)
+    elif args.workload == "aniso_diag_d100":
+        run_gauss(args)
+    elif args.workload == "corr_gauss_d64_full" or args.small or args.dim != 256:
+        run_secondary(args)
     else:
         run_ours(args)
 

@@ -209,3 +209,108 @@ def gauss_adjoint(P, mean, eps, x0, Xi, u, S, objective, Q=None, s=None):
         if gls is not None:
             gls += eps / np.asarray(s) * (Q.T @ lam[:, t]) * (Q.T @ (xb - m))
     return geps, gls
+
+
+# --------------------------------------------------------------------------- batched CPU DEER
+def logistic_batched_model(X, y, tau=1.0):
+    """The batched model functions of bayes_logreg.jl:91-206 (make_problem_batched
+    and make_problem_batched_with_hvp): every call is GEMM -> elementwise -> GEMM
+    through BLAS, as the reference's batched DEER branch calls them.  The softplus
+    is the stable form of docs/src/15-gpu.md:91-97."""
+    X = np.ascontiguousarray(X, np.float64)
+    yc = np.asarray(y, np.float64)[:, None]
+
+    def logp_batch(B):  # bayes_logreg.jl:119-138
+        L = X @ B
+        res = yc * -_softplus(-L) + (1 - yc) * -_softplus(L)
+        return res.sum(axis=0) - 0.5 * tau * (B * B).sum(axis=0)
+
+    def grad_batch(B):  # :140-155
+        L = X @ B
+        return X.T @ (yc - 1.0 / (1.0 + np.exp(-L))) - tau * B
+
+    def hvp_batch(B, V):  # :182-203
+        P = 1.0 / (1.0 + np.exp(-(X @ B)))
+        return -(X.T @ ((P * (1 - P)) * (X @ V))) - tau * V
+
+    return logp_batch, grad_batch, hvp_batch
+
+
+def fwd_and_jvp_batched(model, eps, Xb, Xi, u, Z):
+    """mala_step_batched_fwd_and_jvp! (MALA.jl:556-628), identity mass matrix:
+    gradlogp(X), logp(X), logp(Y), gradlogp(Y), hvp(X, Z), hvp(Y, W) -- twelve
+    GEMMs for the logistic model -- then the column reductions."""
+    logp_b, grad_b, hvp_b = model
+    D = Xb.shape[0]
+    c = np.sqrt(2 * eps)
+    GX = grad_b(Xb)
+    Y = Xb + eps * GX + c * Xi
+    lpX, lpY = logp_b(Xb), logp_b(Y)
+    GY = grad_b(Y)
+    k = (D / 2) * np.log(4 * np.pi * eps)
+    lq_yx = -0.5 * np.sum((Y - (Xb + eps * GX)) ** 2, axis=0) / (2 * eps) - k
+    lq_xy = -0.5 * np.sum((Xb - (Y + eps * GY)) ** 2, axis=0) / (2 * eps) - k
+    la = (lpY + lq_xy) - (lpX + lq_yx)
+    logu = np.log(u)
+    g = 1.0 / (1.0 + np.exp(-(la - logu)))
+    acc = logu < la
+    FT = np.where(acc[None, :], Y, Xb)
+    W = Z + eps * hvp_b(Xb, Z)
+    HvY = hvp_b(Y, W)
+    R = Xb - Y - eps * GY
+    dR = Z - W - eps * HvY
+    dla = np.sum(GY * W, axis=0) - np.sum(GX * Z, axis=0) - (1 / (2 * eps)) * np.sum(R * dR, axis=0)
+    dg = g * (1 - g) * dla
+    Jt = np.where(acc[None, :], W, Z) + (Y - Xb) * dg[None, :]
+    return FT, Jt
+
+
+def scan_doubling(A, B, s0):
+    """solve_affine_scan_diag! (DEERScan.jl:102-173): Hillis-Steele doubling over
+    the maps (a, b), then s_t = a_t s0 + b_t."""
+    a, b = A.copy(), B.copy()
+    T = a.shape[1]
+    off = 1
+    while off < T:
+        an, bn = a.copy(), b.copy()
+        an[:, off:] = a[:, off:] * a[:, :-off]
+        bn[:, off:] = a[:, off:] * b[:, :-off] + b[:, off:]
+        a, b = an, bn
+        off <<= 1
+    return a * np.asarray(s0, float)[:, None] + b
+
+
+def deer_solve_batched(model, eps, s0, Xi, u, probe, *, tol_abs=1e-6, tol_rel=1e-5, maxiter=200,
+                       damping=0.5, chunk=4096):
+    """DEER.solve (DEER.jl:506-595) on the batched :stoch_diag branch with one
+    probe (DEER.jl:398-419): per sweep x_bar = [s0, S[:, :T-1]], Z = probe(iter),
+    (FT, Jt) from fwd_and_jvp_batched over column chunks, A = Z .* Jt,
+    B = FT - A .* x_bar, the doubling scan, damping, and the stopping rule
+    max|dS| <= tol_abs + tol_rel max|S| (:567-578).  Returns (S, info)."""
+    D, T = Xi.shape
+    s0 = np.asarray(s0, np.float64)
+    S = np.repeat(s0[:, None], T, axis=1)
+    Xi = np.asarray(Xi, np.float64)
+    u = np.asarray(u, np.float64)
+    metric, it = np.inf, 0
+    for it in range(1, maxiter + 1):
+        Xbar = np.concatenate([s0[:, None], S[:, :T - 1]], axis=1)
+        Z = probe(it - 1)
+        A = np.empty((D, T))
+        Bm = np.empty((D, T))
+        for c0 in range(0, T, chunk):
+            c1 = min(T, c0 + chunk)
+            FT, Jt = fwd_and_jvp_batched(model, eps, Xbar[:, c0:c1], Xi[:, c0:c1], u[c0:c1],
+                                         Z[:, c0:c1])
+            A[:, c0:c1] = Z[:, c0:c1] * Jt
+            Bm[:, c0:c1] = FT - A[:, c0:c1] * Xbar[:, c0:c1]
+        Sn = scan_doubling(A, Bm, s0)
+        if damping != 1.0:
+            Sn = (1 - damping) * S + damping * Sn
+        metric = np.max(np.abs(Sn - S)) / (tol_abs + tol_rel * np.max(np.abs(Sn)))
+        S = Sn
+        if not np.all(np.isfinite(S)):
+            return S, {"iters": it, "converged": False, "metric": float("nan")}
+        if metric <= 1:
+            return S, {"iters": it, "converged": True, "metric": float(metric)}
+    return S, {"iters": it, "converged": False, "metric": float(metric)}
