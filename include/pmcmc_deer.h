@@ -267,7 +267,11 @@ int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T,
  * whose scratch exceeds the array returns PMCMC_ERR_NOMEM (the scratch needed
  * is about 3 * sizeof(element) * D * ceil(T / tile) bytes, tile <= 64 columns).
  * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Calls share the array: calls that
+ * first call before any stream capture.  The array takes its device memory
+ * when the library's device code is loaded on a device: under lazy module
+ * loading (CUDA_MODULE_LOADING=LAZY, the CUDA 12 default) that is this first
+ * call, so a caller that later hands all free memory to its own pool should
+ * make one call (D = T = 1 will do) before reserving the pool.  Calls share the array: calls that
  * overlap on the GPU (other streams or host threads) race and must be
  * serialised by the caller.  Synchronises `stream` before returning. */
 #define PMCMC_NOALLOC_SCRATCH_BYTES (4u << 20)

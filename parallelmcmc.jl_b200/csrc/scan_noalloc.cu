@@ -16,7 +16,10 @@
 // device and keeps the last call's contents, so each call clears its tile
 // counter and advances a per-device epoch that invalidates stale tile flags;
 // calls that overlap on the GPU (different streams, or several host threads)
-// race on the array and must be serialised by the caller.
+// race on the array and must be serialised by the caller.  The array's memory
+// is taken when the module is loaded on a device, which under lazy loading is
+// the first call there: callers that give every free byte to their own pool
+// make one small call first.
 #include <cuda_runtime.h>
 
 #include <atomic>

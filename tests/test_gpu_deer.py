@@ -10,6 +10,8 @@ Bars (tolerances are written in each test):
 """
 import os
 
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -143,9 +145,16 @@ def test_quickstart_block_matches_oracle_deer_and_sequential(h):
     assert info["iters"] == icpu["iters"] == G["cfg1_deer_iters"][0]
     np.testing.assert_allclose(S, S_cpu, rtol=1e-10, atol=1e-12)  # same algorithm, FP64
     assert np.array_equal(acc, acc_seq)
-    assert trace_err(S, S_seq) < 1e-4
+    # the sampler's default stopping rule (1e-6 + 1e-5 max|S|, DEER.jl:567-578) bounds the
+    # last Newton step; the iterate then sits 2.9e-5 from the sequential trace
+    assert trace_err(S, S_seq) <= 5e-5
     lp_ref = np.array([O.logp(tg, S[:, t]) for t in range(64)])
     np.testing.assert_allclose(lp, lp_ref, rtol=1e-12, atol=1e-12)
+    # a rule ten times tighter meets the 1e-5 trace bar
+    tight = dataclasses.replace(sampler, tol_abs=1e-7, tol_rel=1e-6)
+    S2, info2, _, acc2 = _run(h, model, tight, x0, 0, 0)
+    assert info2["converged"] and np.array_equal(acc2, acc_seq)
+    assert trace_err(S2, S_seq) <= 1e-5
 
 
 def test_diag_jacobian_recovers_sequential(h):
@@ -336,9 +345,29 @@ def test_sample_quickstart_matches_fixture(h):
     assert np.array_equal(ch.accepted, G["cfg1_seq_accept"])
     # same algorithm in FP64 on the same tape and probes as the oracle's CPU DEER
     np.testing.assert_allclose(ch.values.T, G["cfg1_deer_values"], rtol=1e-9, atol=1e-11)
-    assert trace_err(ch.values.T, G["cfg1_seq_values"]) < 1e-3
+    # the fixture's sequential trace restarts every block from the DEER hand-off
+    assert trace_err(ch.values.T, G["cfg1_seq_values"]) <= 3e-4
     assert ch.info["converged"] == 1
     assert ch.info["iters"] == int(np.sum(G["cfg1_deer_iters"]))
+
+
+def test_sample_quickstart_matches_one_sequential_chain(h):
+    # the same 500 samples at a tighter stopping rule against one FP64 sequential chain
+    # over all 500 steps (tape block b for steps 64 b .. 64 b + 63)
+    model, sampler, x0, meta = configs.quickstart_2d()
+    tight = dataclasses.replace(sampler, tol_abs=1e-8, tol_rel=1e-7)
+    ch = pmcmc.sample(model, tight, 500, seed=0, initial_params=x0, handle=h)
+    tg = _oracle_target(model)
+    x, seq, accs = np.asarray(x0, np.float64), [], []
+    for b in range(8):
+        Xi, u = O.tape(0, b, 2, 64)
+        S_b, a_b, _ = O.mala_sequential(tg, 0.1, x, Xi, u)
+        seq.append(S_b)
+        accs.append(a_b)
+        x = S_b[:, -1].copy()
+    S_seq = np.concatenate(seq, axis=1)[:, :500]
+    assert np.array_equal(ch.accepted, np.concatenate(accs)[:500])
+    assert trace_err(ch.values.T, S_seq) <= 1e-5
 
 
 def test_sample_device_tensors_match_host(h):

@@ -37,3 +37,35 @@ def test_fleet_reports_a_failing_chain():
     chains[1] = (model, bad, x0, seed, block)
     with pytest.raises(pmcmc.ArgumentError):
         pmcmc.fleet_solve(chains, workers=2)
+
+
+def test_fleet_chains_match_the_fp64_sequential_chains():
+    """Chains of the uneven fleet distribution (D on both tensor-core passes) solved
+    together, each against its own FP64 sequential chain on the same tape
+    (MALA.jl:322-346): identical accepts, trace error at most 1e-5."""
+    import dataclasses
+
+    import oracle as O
+    chains = configs.logistic_fleet(n_chains=6, scale=0.05)
+    # the FP32-state stopping rule of the 1e-5 trace bar (1e-7 + 1e-6 max|S|); a rule ten
+    # times tighter sits at the FP32 rounding floor
+    chains = [(m, dataclasses.replace(s, tol_abs=1e-7, tol_rel=1e-6, maxiter=400), x0, sd, b)
+              for m, s, x0, sd, b in chains]
+    assert any(m.dim > 256 for m, *_ in chains) and any(m.dim <= 256 for m, *_ in chains)
+    fleet = pmcmc.fleet_solve(chains, workers=3, handle=pmcmc.Handle(0), errors="report")
+    checked = 0
+    for (model, sampler, x0, seed, block), (S, info, lp, acc) in zip(chains, fleet):
+        if info["status"]:  # stiff chains that DEER itself cannot solve are reported
+            continue
+        assert info["converged"], info
+        tg = O.Target.logistic(model.target["X"], model.target["y"])
+        Xi, u = O.tape(seed, block, model.dim, sampler.T)
+        S_seq, acc_seq, _ = O.mala_sequential_logistic(tg, sampler.epsilon, np.zeros(model.dim),
+                                                       Xi, u)
+        assert np.array_equal(np.asarray(acc, bool), acc_seq), (seed, model.dim)
+        S = np.asarray(S, np.float64)
+        err = np.max(np.linalg.norm(S - S_seq, axis=0) /
+                     np.maximum(np.linalg.norm(S_seq, axis=0), 1e-30))
+        assert err <= 1e-5, (seed, model.dim, err)
+        checked += 1
+    assert checked >= 4
