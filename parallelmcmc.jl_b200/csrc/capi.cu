@@ -366,7 +366,7 @@ struct SolveLayout {
   size_t S0, S1, x0a, x0b, flags, agg_a, agg_b, incl, colmax, out_S, out_lp, out_acc;
   size_t pA, pB, al0, be0, al1, be1, red;  // plain path only
   size_t lg[5], lpx, lpy, acc_col, la_col, Bb, Lb, Gb;  // logistic only
-  size_t la_ref, tie;                                   // logistic: log alpha, near-tie scratch
+  size_t la_ref, tie, lg_acc;                           // logistic: log alpha, near-tie scratch, probe sum
   size_t xi, logu;
   size_t tcws, Gtc;  // tensor-core logistic path
   size_t fU, fV, fR, facc, fPhi, fbeta, fdin, fpart, eS0, eS1, exi, ex0;  // :full mode
@@ -427,6 +427,7 @@ SolveLayout layout(int64_t D, int64_t Dp, int64_t T, int ntiles, size_t es, bool
     L.Gb = take(es * Dp * 2 * Tc);
     L.la_ref = take(8 * static_cast<size_t>(T));
     L.tie = take(tie_bytes);
+    L.lg_acc = take(es * T * Dp);
   }
   if (tc_bytes) {
     L.tcws = take(tc_bytes);
@@ -715,6 +716,8 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   double* la_ref = reinterpret_cast<double*>(ws + L.la_ref);
   const TieBufs tb = lg_tie_carve(ws + L.tie, tg->lg, P.T, tie_kmax(P.T));
   P.la_ref = refine ? la_ref : nullptr;
+  P.lg_acc = ws + L.lg_acc;
+  const void* k_acc = k.eval;  // the probe accumulation kernel of the logistic target
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(coop ? k.sweep_coop : k.sweep), smem_sweep));
@@ -732,24 +735,25 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   void *Bb = ws + L.Bb, *Lb = ws + L.Lb, *Gb = ws + L.Gb;
   int* tc_err = use_tc ? lg_tc_err_word(ws + L.tcws, tg->lg, P.T) : nullptr;
   if (use_tc) CK(cudaMemsetAsync(tc_err, 0, sizeof(int), h->stream));
-  auto pass_impl = [&](int mode, double* lp) -> int {
+  auto pass_impl = [&](int mode, double* lp, int probe) -> int {
     if (use_tc) {
       float* G = reinterpret_cast<float*>(ws + L.Gtc);
-      if (lg_tc_pass(h->stream, tg->lg, h->d_params, h->d_state, lp, mode, P.T, ws + L.tcws, G))
+      if (lg_tc_pass(h->stream, tg->lg, h->d_params, h->d_state, lp, mode, P.T, ws + L.tcws, G,
+                     probe))
         return 1;
       if (mode != 2 && lg_mid(h->stream, false, h->d_params, h->d_state, mode + 1, 0,
-                              static_cast<int>(P.T), P.Dp, G) != cudaSuccess)
+                              static_cast<int>(P.T), probe, P.Dp, G) != cudaSuccess)
         return 1;
       return 0;
     }
     return lg_plain_pass(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, lp, mode,
-                         P.T, P.Dp, Bb, Lb, Gb, Tc);
+                         P.T, P.Dp, Bb, Lb, Gb, Tc, probe);
   };
-  auto pass = [&](int mode, double* lp) -> int {
+  auto pass = [&](int mode, double* lp, int probe = 0) -> int {
     if (h->profiling && mode != 2) {
       // one contraction pass timed on its own (events around it, synchronised)
       if (cudaEventRecord(h->ev[0], h->stream) != cudaSuccess) return 1;
-      const int rc = pass_impl(mode, lp);
+      const int rc = pass_impl(mode, lp, probe);
       float ms = 0;
       if (rc || cudaEventRecord(h->ev[1], h->stream) != cudaSuccess ||
           cudaEventSynchronize(h->ev[1]) != cudaSuccess ||
@@ -759,7 +763,7 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
       h->prof.pass_ms += ms;
       return 0;
     }
-    return pass_impl(mode, lp);
+    return pass_impl(mode, lp, probe);
   };
   auto tie = [&]() -> int {
     if (lg_tie_refine(h->stream, h->cublas, tg->lg, f64, h->d_params, h->d_state, P.T, la_ref,
@@ -771,16 +775,26 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   // the tensor-core error word travels with the state in every per-sweep copy
   int* h_err = reinterpret_cast<int*>(h->h_red + 3);
   *h_err = 0;
+  // probes > 1 (DEER.jl:412-418): the passes run once per probe; the probes before the
+  // last add z_k .* J z_k into lg_acc, the sweep adds the last and divides
+  const int grid_acc = static_cast<int>(std::min<int64_t>((P.T + kWarps - 1) / kWarps,
+                                                          int64_t(h->num_sms) * 8));
   for (int it = 0; it < P.maxiter; ++it) {
-    if (pass(0, P.lpx))
-      return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
-                  cudaGetErrorString(cudaGetLastError()));
-    if (pass(1, P.lpy))
-      return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
-                  cudaGetErrorString(cudaGetLastError()));
-    if (refine) {
-      const int rc = tie();
-      if (rc) return rc;
+    for (int pr = 0; pr < P.probes; ++pr) {
+      if (pass(0, P.lpx, pr))
+        return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      if (pass(1, P.lpy, pr))
+        return fail(h, PMCMC_ERR_CUDA, "logistic pass 2 failed: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      if (refine && pr == 0) {  // the value columns, and so log alpha, are the same for every probe
+        const int rc = tie();
+        if (rc) return rc;
+      }
+      if (pr + 1 < P.probes) {
+        void* acc_args[] = {&h->d_params, &h->d_state, &pr};
+        CK(cudaLaunchKernel(k_acc, dim3(grid_acc), dim3(kThreads), acc_args, 0, h->stream));
+      }
     }
     if (h->profiling) CK(cudaEventRecord(h->ev[0], h->stream));
     CK(launch_sweep(coop ? k.sweep_coop : k.sweep, coop, P.ntiles, smem_sweep, sweep_args,
@@ -1179,8 +1193,6 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (tg->kind == kLogistic) {
     if (p->jacobian != PMCMC_JAC_STOCH_DIAG)
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: only :stoch_diag is built");
-    if (p->probes != 1)
-      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: probes must be 1");
     if (p->window > 0 && p->window < p->T)
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: no sliding window");
   }

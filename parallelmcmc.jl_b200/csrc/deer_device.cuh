@@ -61,6 +61,8 @@ struct DevParams {
   // log alpha of every column with near-tie columns recomputed in FP64
   // (logistic_tie.cu); nullptr: the sweep forms log alpha itself
   const double* la_ref;
+  // probes > 1: sum of z_k .* J z_k over the probes 0 .. probes-2 of the sweep (T x Dp, Real)
+  void* lg_acc;
   double tau;  // prior precision
   // tape of the block, written once by the init kernel: xi (T x Dp, FP32,
   // padded rows zero) and log(u_t) in FP64

@@ -17,7 +17,8 @@ struct SweepKernels {
   const void* sweep_coop = nullptr;  // same signature, cooperative launch (all tiles resident)
   const void* finalize = nullptr;  // (const DevParams*, DevState*)
   const void* init = nullptr;      // (const DevParams*, DevState*)
-  const void* eval = nullptr;      // (const DevParams*, const Real* Sold, int iter, int from_x0, Real* A, Real* B)
+  const void* eval = nullptr;      // (const DevParams*, const Real* Sold, int iter, int from_x0, Real* A, Real* B);
+                                   // logistic: the probe accumulation (const DevParams*, const DevState*, int probe)
   const void* persist = nullptr;   // (const DevParams*, DevState*): whole solve, cooperative
   int qpl = 1;
 };

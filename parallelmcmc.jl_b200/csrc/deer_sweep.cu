@@ -30,10 +30,14 @@ namespace pmcmc {
 // Logistic target: the gradient / HVP contractions over the N data rows come
 // from the two GEMM passes of this sweep (g_x, y, w, g_y, H(y) w in HBM,
 // likelihood sums in FP64); this evaluates the rest of the batched
-// fwd + JVP (MALA.jl:592-625) for one column and returns A and B.
+// fwd + JVP (MALA.jl:592-625) for one column, probe `probe`, and returns
+// A = scale * (z .* J z + acc_in) and B = F - A .* x_bar: with several
+// probes, acc_in holds the earlier probes' z .* J z and scale is 1 / probes
+// (the probe average of DEER.jl:412-418).
 template <typename Real, int QPL>
 __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKey& key,
-                                                const Real* xcol, int t, int iter,
+                                                const Real* xcol, int t, int iter, int probe,
+                                                const Real* acc_in, Real scale,
                                                 Real (&A)[QPL][4], Real (&Bv)[QPL][4]) {
   const int lane = threadIdx.x & 31;
   const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
@@ -58,8 +62,8 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
       load4(hvp + 4 * j, hvy[q]);
       float xi[4];
       load4(P.xi + off + 4 * j, xi);
-      const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t), 0,
-                               iter);
+      const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t),
+                               probe, iter);
       const uint32_t wv = u4_word(pb, (j >> 3) & 3);
       const int sh = (j & 7) * 4;
 #pragma unroll
@@ -98,14 +102,18 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
   dla = warp_sum(dla);
   const Real dg = gp * dla;
 #pragma unroll
-  for (int q = 0; q < QPL; ++q)
+  for (int q = 0; q < QPL; ++q) {
+    Real prev[4] = {Real(0), Real(0), Real(0), Real(0)};
+    const int j = lane + 32 * q;
+    if (acc_in && 4 * j < D) load4(acc_in + off + 4 * j, prev);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const Real jz = (acc ? w[q][e] : z[q][e]) + (y[q][e] - x[q][e]) * dg;
-      A[q][e] = z[q][e] * jz;
+      A[q][e] = scale * (z[q][e] * jz + prev[e]);
       const Real f = acc ? y[q][e] : x[q][e];
       Bv[q][e] = f - A[q][e] * x[q][e];
     }
+  }
   if (lane == 0) {
     P.acc_col[t] = acc ? 1 : 0;
     P.la_col[t] = la - logu;
@@ -207,7 +215,12 @@ __global__ void __launch_bounds__(kThreads)
       const int t = static_cast<int>(t0 + c);
       Real A[QPL][4], Bq[QPL][4];
       if constexpr (TK == kLogistic) {
-        column_logistic<Real, QPL>(P, key, sm.Xs + c * Dp, t, iter, A, Bq);
+        // the last probe of the sweep; the earlier ones are in lg_acc
+        const bool multi = P.probes > 1;
+        column_logistic<Real, QPL>(P, key, sm.Xs + c * Dp, t, iter, P.probes - 1,
+                                   multi ? static_cast<const Real*>(P.lg_acc) : nullptr,
+                                   multi ? Real(1) / static_cast<Real>(P.probes) : Real(1), A,
+                                   Bq);
       } else {
         float xic[QPL][4];
 #pragma unroll
@@ -637,6 +650,45 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Logistic target with probes > 1: after the passes of probe k < probes - 1,
+// lg_acc += z_k .* J z_k (lg_acc = for k = 0), one warp a column.  The last
+// probe is added, and the sum divided by the probe count, in the sweep.
+// ---------------------------------------------------------------------------
+template <typename Real, int QPL>
+__global__ void __launch_bounds__(kThreads)
+    lg_probe_accum_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
+                          int probe) {
+  __shared__ DevParams P;
+  load_params(Pg, P);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int Dp = static_cast<int>(P.Dp), D = static_cast<int>(P.D);
+  const int iter = st->iter;
+  const bool from_x0 = iter == 0;
+  const Real* S = static_cast<const Real*>(P.S[st->cur]);
+  const Real* x0 = static_cast<const Real*>(P.x0);
+  Real* accv = static_cast<Real*>(P.lg_acc);
+  const TapeKey key(P.seed, P.block);
+  for (int64_t t = static_cast<int64_t>(blockIdx.x) * kWarps + warp; t < P.T;
+       t += static_cast<int64_t>(gridDim.x) * kWarps) {
+    const Real* xcol = (from_x0 || t == 0) ? x0 : S + (t - 1) * Dp;
+    Real A[QPL][4], Bq[QPL][4];
+    column_logistic<Real, QPL>(P, key, xcol, static_cast<int>(t), iter, probe,
+                               probe > 0 ? accv : nullptr, Real(1), A, Bq);
+#pragma unroll
+    for (int q = 0; q < QPL; ++q) {
+      const int j = lane + 32 * q;
+      if (4 * j < D) {
+        Real a4[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) a4[e] = (4 * j + e < D) ? A[q][e] : Real(0);
+        store4(accv + t * Dp + 4 * j, a4);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Logistic finalize: copy the kept columns out, logp(S_t) from the likelihood
 // sums of the last logp pass (left in lpx) plus the prior, and the accept
 // flags / margins of acc_col / la_col: those of the verification pass at the
@@ -731,7 +783,7 @@ static SweepKernels pick_logistic() {
   k.sweep_coop = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL, true>);
   k.finalize = reinterpret_cast<const void*>(&deer_finalize_logistic_kernel<Real>);
   k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
-  k.eval = nullptr;
+  k.eval = reinterpret_cast<const void*>(&lg_probe_accum_kernel<Real, QPL>);
   return k;
 }
 

@@ -26,13 +26,14 @@ namespace pmcmc {
 // ---------------------------------------------------------------------------
 
 // B (Dp x ncols, column-major) for a column chunk [t0, t0+Tc):
-//   mode 0: [x_bar_t | z_t]   (x_bar_t = S_{t-1}, or x0 at t = 0 / first sweep)
+//   mode 0: [x_bar_t | z_t]   (x_bar_t = S_{t-1}, or x0 at t = 0 / first sweep; z_t the
+//                              Rademacher probe `probe` of this sweep)
 //   mode 1: [y_t | w_t]
 //   mode 2: [S_t]             (logp of the returned trajectory)
 // and zero the likelihood accumulators of the chunk.
 template <typename Real>
 __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
-                               int mode, int64_t t0, int Tc, Real* __restrict__ B) {
+                               int mode, int64_t t0, int Tc, int probe, Real* __restrict__ B) {
   const DevParams& P = *Pg;
   const int64_t Dp = P.Dp, D = P.D;
   const int iter = st->iter;
@@ -56,7 +57,7 @@ __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
           v = (from_x0 || t == 0) ? x0[d] : S[(t - 1) * Dp + d];
         } else {
           const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t),
-                                   0, iter);
+                                   probe, iter);
           v = ((u4_word(pb, static_cast<int>((d >> 5) & 3)) >> (d & 31)) & 1u) ? Real(1)
                                                                               : Real(-1);
         }
@@ -114,7 +115,7 @@ __global__ void lg_epilogue_kernel(const Real* __restrict__ ylab, int64_t N, int
 // G is Dp x 2Tc column-major (value block then tangent block).
 template <typename Real>
 __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
-                              int stage, int64_t t0, int Tc, const Real* __restrict__ G) {
+                              int stage, int64_t t0, int Tc, int probe, const Real* __restrict__ G) {
   const DevParams& P = *Pg;
   const int64_t Dp = P.Dp, D = P.D;
   const int64_t nq = Dp / 4;
@@ -144,8 +145,8 @@ __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* 
         xi[2] = v.z;
         xi[3] = v.w;
       }
-      const U4 pb = probe_bits(key, static_cast<uint32_t>(q >> 5), static_cast<uint32_t>(t), 0,
-                               iter);
+      const U4 pb = probe_bits(key, static_cast<uint32_t>(q >> 5), static_cast<uint32_t>(t),
+                               probe, iter);
       const uint32_t wv = u4_word(pb, static_cast<int>((q >> 3) & 3));
       const int sh = static_cast<int>(q & 7) * 4;
 #pragma unroll
@@ -197,11 +198,13 @@ static int grid_for(int64_t n) {
 }
 
 cudaError_t lg_prep(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS, int mode,
-                    int64_t t0, int Tc, int64_t Dp, void* B) {
+                    int64_t t0, int Tc, int probe, int64_t Dp, void* B) {
   const int ncols = mode == 2 ? Tc : 2 * Tc;
   const int g = grid_for(static_cast<int64_t>(ncols) * Dp);
-  if (f64) lg_prep_kernel<double><<<g, 256, 0, s>>>(dP, dS, mode, t0, Tc, static_cast<double*>(B));
-  else lg_prep_kernel<float><<<g, 256, 0, s>>>(dP, dS, mode, t0, Tc, static_cast<float*>(B));
+  if (f64)
+    lg_prep_kernel<double><<<g, 256, 0, s>>>(dP, dS, mode, t0, Tc, probe, static_cast<double*>(B));
+  else
+    lg_prep_kernel<float><<<g, 256, 0, s>>>(dP, dS, mode, t0, Tc, probe, static_cast<float*>(B));
   return cudaGetLastError();
 }
 
@@ -219,12 +222,14 @@ cudaError_t lg_epilogue(cudaStream_t s, bool f64, const void* ylab, int64_t N, i
 }
 
 cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS, int stage,
-                   int64_t t0, int Tc, int64_t Dp, const void* G) {
+                   int64_t t0, int Tc, int probe, int64_t Dp, const void* G) {
   const int g = grid_for(static_cast<int64_t>(Tc) * (Dp / 4));
   if (f64)
-    lg_mid_kernel<double><<<g, 256, 0, s>>>(dP, dS, stage, t0, Tc, static_cast<const double*>(G));
+    lg_mid_kernel<double><<<g, 256, 0, s>>>(dP, dS, stage, t0, Tc, probe,
+                                            static_cast<const double*>(G));
   else
-    lg_mid_kernel<float><<<g, 256, 0, s>>>(dP, dS, stage, t0, Tc, static_cast<const float*>(G));
+    lg_mid_kernel<float><<<g, 256, 0, s>>>(dP, dS, stage, t0, Tc, probe,
+                                           static_cast<const float*>(G));
   return cudaGetLastError();
 }
 
@@ -232,12 +237,12 @@ cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState
 // mode 0/1 = pass 1/2 (mid stage 1/2), mode 2 = logp pass (no tangent, no mid).
 int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
                   const DevParams* dP, const DevState* dS, double* lp, int mode, int64_t T,
-                  int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc) {
+                  int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc, int probe) {
   const int64_t N = X.N;
   for (int64_t t0 = 0; t0 < T; t0 += Tc) {
     const int tc = static_cast<int>(Tc);
     const int ncols = mode == 2 ? tc : 2 * tc;
-    if (lg_prep(s, f64, dP, dS, mode, t0, tc, Dp, Bbuf) != cudaSuccess) return 3;
+    if (lg_prep(s, f64, dP, dS, mode, t0, tc, probe, Dp, Bbuf) != cudaSuccess) return 3;
     cublasStatus_t st;
     if (f64) {
       const double one = 1.0, zero = 0.0;
@@ -274,7 +279,7 @@ int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool 
                        static_cast<float*>(Gbuf), static_cast<int>(Dp));
     }
     if (st != CUBLAS_STATUS_SUCCESS) return 3;
-    if (lg_mid(s, f64, dP, dS, mode + 1, t0, tc, Dp, Gbuf) != cudaSuccess) return 3;
+    if (lg_mid(s, f64, dP, dS, mode + 1, t0, tc, probe, Dp, Gbuf) != cudaSuccess) return 3;
   }
   return 0;
 }

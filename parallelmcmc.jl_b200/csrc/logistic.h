@@ -27,12 +27,13 @@ struct LogisticDev {
 };
 
 int64_t lg_chunk_cols(int64_t N, int64_t T);
+// `probe` picks the Rademacher probe of the tangent columns (mode 0; DEER.jl:412-416).
 int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
                   const DevParams* dP, const DevState* dS, double* lp, int mode, int64_t T,
-                  int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc);
+                  int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc, int probe);
 
 cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS, int stage,
-                   int64_t t0, int Tc, int64_t Dp, const void* G);
+                   int64_t t0, int Tc, int probe, int64_t Dp, const void* G);
 
 // Tensor-core pass (logistic_tc.cu): mode 0/1/2 as in lg_plain_pass; writes G
 // (Dp x 2T FP32, value block then tangent block) and lp.  ws holds the FP16
@@ -40,7 +41,7 @@ cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState
 bool lg_tc_supported(const LogisticDev& X);
 size_t lg_tc_ws_bytes(const LogisticDev& X, int64_t T);
 int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const DevState* dS,
-               double* lp, int mode, int64_t T, void* ws, float* G);
+               double* lp, int mode, int64_t T, void* ws, float* G, int probe);
 int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T);
 // One bounded mbarrier wait that nothing completes (bound check); err[0] = 1
 // when it gave up.

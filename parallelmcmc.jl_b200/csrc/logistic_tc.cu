@@ -515,11 +515,11 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 
 // Builds the FP16 split operands of one pass: Bh/Bl (value columns hi / lo)
 // and Bt (tangent columns), each T x Dk (t-major rows, d contiguous).
-//   mode 0: value x_bar_t, tangent z_t; mode 1: value y_t, tangent w_t;
+//   mode 0: value x_bar_t, tangent z_t (probe `probe`); mode 1: value y_t, tangent w_t;
 //   mode 2: value S_t, no tangent.
 template <typename Real>
 __global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
-                               int mode, int64_t Dk, __half* __restrict__ Bh,
+                               int mode, int probe, int64_t Dk, __half* __restrict__ Bh,
                                __half* __restrict__ Bl, __half* __restrict__ Bt) {
   const DevParams& P = *Pg;
   const int iter = st->iter;
@@ -535,8 +535,8 @@ __global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
     if (d < P.D) {
       if (mode == 0) {
         v = static_cast<float>((from_x0 || t == 0) ? x0[d] : S[(t - 1) * P.Dp + d]);
-        const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t), 0,
-                                 iter);
+        const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t),
+                                 probe, iter);
         tv = ((u4_word(pb, static_cast<int>((d >> 5) & 3)) >> (d & 31)) & 1u) ? 1.f : -1.f;
       } else if (mode == 1) {
         v = static_cast<float>(static_cast<const Real*>(P.lg[1])[t * P.Dp + d]);
@@ -968,7 +968,7 @@ int* lg_tc_err_word(void* ws, const LogisticDev& X, int64_t T) {
 }
 
 int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const DevState* dS,
-               double* lp, int mode, int64_t T, void* ws, float* G_out) {
+               double* lp, int mode, int64_t T, void* ws, float* G_out, int probe) {
   const int64_t Dk = X.Dk;
   __half* Bh = static_cast<__half*>(ws);
   __half* Bl = Bh + T * Dk;
@@ -976,7 +976,7 @@ int lg_tc_pass(cudaStream_t s, const LogisticDev& X, const DevParams* dP, const 
   float* G = G_out;
   int* err = lg_tc_err_word(ws, X, T);
   const int g = static_cast<int>((T * Dk + 255) / 256 < 148 * 16 ? (T * Dk + 255) / 256 : 148 * 16);
-  tc::tc_prep_kernel<float><<<g, 256, 0, s>>>(dP, dS, mode, Dk, Bh, Bl, Bt);
+  tc::tc_prep_kernel<float><<<g, 256, 0, s>>>(dP, dS, mode, probe, Dk, Bh, Bl, Bt);
   if (cudaGetLastError() != cudaSuccess) return 3;
   CUtensorMap mXh, mXl, mBh, mBl, mBt;
   if (!make_map(&mXh, X.Xh, X.Np, Dk, tc::BN) || !make_map(&mXl, X.Xl, X.Np, Dk, tc::BN) ||

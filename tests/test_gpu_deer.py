@@ -522,6 +522,37 @@ def test_logistic_deer_iterations_match_cpu_deer(h):
     np.testing.assert_allclose(S, S_cpu, rtol=1e-9, atol=1e-10)
 
 
+@pytest.mark.parametrize("probes", [2, 3])
+def test_logistic_probes_match_cpu_deer(h, probes):
+    # Hutchinson with several probes, averaged as DEER.jl:412-418 does: the FP64 path
+    # takes the oracle's iterates, sweep for sweep, on the same probes
+    N, D, T, eps = 250, 10, 96, 0.02
+    X, y = _logistic_problem(N, D, 35)
+    model = pmcmc.DensityModel.logistic(X, y)
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", probes=probes,
+                                        dtype=np.float64, exec="plain")
+    S, info = pmcmc.solve(model, sampler, np.zeros(D), seed=12, handle=h)
+    Xi, u = O.tape(12, 0, D, T)
+    S_cpu, icpu = O.deer_solve(O.Target.logistic(X, y), eps, np.zeros(D), Xi, u, 12, 0,
+                               probes=probes)
+    assert info["iters"] == icpu["iters"]
+    np.testing.assert_allclose(S, S_cpu, rtol=1e-9, atol=1e-10)
+
+
+def test_logistic_probes_on_tensor_cores_match_sequential(h):
+    N, D, T, eps = 600, 96, 160, 0.02
+    X, y = _logistic_problem(N, D, 36)
+    model = pmcmc.DensityModel.logistic(X, y)
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="stoch_diag", probes=3,
+                                        dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6)
+    S, info, lp, acc = _run(h, model, sampler, np.zeros(D, np.float32), 13, 0)
+    Xi, u = O.tape(13, 0, D, T)
+    S_seq, acc_seq, _ = O.mala_sequential(O.Target.logistic(X, y), eps, np.zeros(D), Xi, u)
+    assert info["converged"] and "tensor_core" in info["path_names"], info
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= 1e-5
+
+
 def test_logistic_unsupported_modes(h):
     X, y = _logistic_problem(50, 4, 33)
     model = pmcmc.DensityModel.logistic(X, y)
