@@ -779,8 +779,19 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   // last add z_k .* J z_k into lg_acc, the sweep adds the last and divides
   const int grid_acc = static_cast<int>(std::min<int64_t>((P.T + kWarps - 1) / kWarps,
                                                           int64_t(h->num_sms) * 8));
+  const bool lg_diag = P.jac == PMCMC_JAC_DIAG;
   for (int it = 0; it < P.maxiter; ++it) {
-    for (int pr = 0; pr < P.probes; ++pr) {
+    // exact diagonal: g_x, y, diag H_x | g_y | H_y r | H_x u (logistic.cu, modes 3-6)
+    for (int m = 3; lg_diag && m <= 6; ++m) {
+      if (pass(m, m == 4 || m == 5 ? P.lpy : P.lpx))
+        return fail(h, PMCMC_ERR_CUDA, "logistic :diag pass failed: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      if (refine && m == 4) {
+        const int rc = tie();
+        if (rc) return rc;
+      }
+    }
+    for (int pr = 0; !lg_diag && pr < P.probes; ++pr) {
       if (pass(0, P.lpx, pr))
         return fail(h, PMCMC_ERR_CUDA, "logistic pass 1 failed: %s",
                     cudaGetErrorString(cudaGetLastError()));
@@ -1191,8 +1202,8 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
   if (N < 1) return fail(h, PMCMC_ERR_ARGUMENT, "the number of samples must be >= 1");
   if (tg->kind == kLogistic) {
-    if (p->jacobian != PMCMC_JAC_STOCH_DIAG)
-      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: only :stoch_diag is built");
+    if (p->jacobian == PMCMC_JAC_FULL)
+      return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: :full is not built");
     if (p->window > 0 && p->window < p->T)
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: no sliding window");
   }
@@ -1222,7 +1233,7 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
     rc = ensure_eigen(h, const_cast<pmcmc_target*>(tg));
     if (rc) return rc;
   }
-  const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D)
+  const SweepKernels k = logistic ? logistic_sweep_kernels(f64, D, p->jacobian)
                                   : gauss_sweep_kernels(f64, tg->kind, p->jacobian, D);
   // whole solve in one cooperative launch when every tile is co-resident
   const int TTp = (!plain && !logistic && !full && W == T && !h->force_eager && !h->no_persist)
@@ -1240,7 +1251,16 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   if (sp_sweep.total > 200 * 1024)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "dimension %lld too large for the fused sweep",
                 (long long)D);
-  const bool use_tc = logistic && !plain && !f64 && lg_tc_supported(tg->lg);
+  // the exact diagonal contracts X .* X, which the tensor-core pass has no operand for
+  const bool lg_diag = logistic && p->jacobian == PMCMC_JAC_DIAG;
+  const bool use_tc = logistic && !plain && !f64 && !lg_diag && lg_tc_supported(tg->lg);
+  if (lg_diag) {
+    static std::mutex square_mu;  // targets are shared by the fleet's worker threads
+    std::lock_guard<std::mutex> lk(square_mu);
+    auto& lgd = const_cast<pmcmc_target*>(tg)->lg;
+    CK(lg_make_square(h->stream, lgd, f64));
+    CK(cudaStreamSynchronize(h->stream));
+  }
   const int64_t Tc = logistic && !use_tc ? std::min<int64_t>(T, lg_chunk_cols(tg->N, T)) : 0;
   const int64_t nblocks = (N + T - 1) / T;
   // Host outputs of several blocks: block b's copy-out overlaps block b + 1's solve.
@@ -1768,6 +1788,8 @@ int pmcmc_target_destroy(pmcmc_target* t) {
   cudaFree(t->lg.y64);
   cudaFree(t->lg.Xh);
   cudaFree(t->lg.Xl);
+  cudaFree(t->lg.X2_32);
+  cudaFree(t->lg.X2_64);
   for (void* q : {static_cast<void*>(t->lam_f), static_cast<void*>(t->qrm_f),
                   static_cast<void*>(t->qcm_f), static_cast<void*>(t->lamq_f),
                   static_cast<void*>(t->lamq_d), static_cast<void*>(t->zq_f),

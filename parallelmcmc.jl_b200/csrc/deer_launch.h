@@ -38,7 +38,7 @@ const void* persist_kernel(bool f64, int tk, int jac, int64_t D);
 cudaError_t raise_smem_limit(const void* fn, size_t bytes);
 
 SweepKernels gauss_sweep_kernels(bool f64, int tk, int jac, int64_t D);
-SweepKernels logistic_sweep_kernels(bool f64, int64_t D);
+SweepKernels logistic_sweep_kernels(bool f64, int64_t D, int jac);
 SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);
 
 // Independent sequential MALA chains, one warp a chain (mala_chains.cu): chain c

@@ -120,6 +120,66 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
   }
 }
 
+// Logistic target, exact diagonal (:diag): J_ii = a (1 + eps H_x,ii) + (1 - a)
+// + (y - x_bar)_i g' dla_i, with diag H_x in lg[2] and dla in lg[4] from the
+// four passes of the sweep (logistic.cu, stages 3-6); A and B for one column.
+template <typename Real, int QPL>
+__device__ __forceinline__ void column_logistic_diag(const DevParams& P, const Real* xcol, int t,
+                                                     Real (&A)[QPL][4], Real (&Bv)[QPL][4]) {
+  const int lane = threadIdx.x & 31;
+  const int D = static_cast<int>(P.D), Dp = static_cast<int>(P.Dp);
+  const Real eps = static_cast<Real>(P.eps);
+  const size_t off = static_cast<size_t>(t) * Dp;
+  const Real* yp = static_cast<const Real*>(P.lg[1]) + off;
+  const Real* hdp = static_cast<const Real*>(P.lg[2]) + off;
+  const Real* gyp = static_cast<const Real*>(P.lg[3]) + off;
+  const Real* dlp = static_cast<const Real*>(P.lg[4]) + off;
+  Real x[QPL][4], y[QPL][4], hd[QPL][4], dl[QPL][4];
+  double la = 0.0;
+#pragma unroll
+  for (int q = 0; q < QPL; ++q) {
+    const int j = lane + 32 * q;
+    if (4 * j < D) {
+      Real gy[4];
+      float xi[4];
+      load4(xcol + 4 * j, x[q]);
+      load4(yp + 4 * j, y[q]);
+      load4(hdp + 4 * j, hd[q]);
+      load4(dlp + 4 * j, dl[q]);
+      load4(gyp + 4 * j, gy);
+      load4(P.xi + off + 4 * j, xi);
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * j + e < D) {
+          const double xd = static_cast<double>(x[q][e]), yd = static_cast<double>(y[q][e]);
+          const double r1 = P.sqrt2eps * static_cast<double>(xi[e]);
+          const double r2 = (xd - yd) - P.eps * static_cast<double>(gy[e]);
+          la += -0.5 * P.tau * (yd * yd - xd * xd) + (r1 * r1 - r2 * r2) * P.inv4eps;
+        }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) x[q][e] = y[q][e] = hd[q][e] = dl[q][e] = Real(0);
+    }
+  }
+  la = warp_sum(la) + (P.lpy[t] - P.lpx[t]);
+  if (P.la_ref) la = P.la_ref[t];
+  const double logu = P.logu[t];
+  const bool acc = logu < la;
+  const Real gp = sigmoid_slope<Real>(la - logu);
+#pragma unroll
+  for (int q = 0; q < QPL; ++q)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      A[q][e] = (acc ? Real(1) + eps * hd[q][e] : Real(1)) + (y[q][e] - x[q][e]) * gp * dl[q][e];
+      const Real f = acc ? y[q][e] : x[q][e];
+      Bv[q][e] = f - A[q][e] * x[q][e];
+    }
+  if (lane == 0) {
+    P.acc_col[t] = acc ? 1 : 0;
+    P.la_col[t] = la - logu;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // The sweep kernel
 // ---------------------------------------------------------------------------
@@ -214,7 +274,9 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = warp; c < ncols; c += kWarps) {
       const int t = static_cast<int>(t0 + c);
       Real A[QPL][4], Bq[QPL][4];
-      if constexpr (TK == kLogistic) {
+      if constexpr (TK == kLogistic && JAC == kJacDiag) {
+        column_logistic_diag<Real, QPL>(P, sm.Xs + c * Dp, t, A, Bq);
+      } else if constexpr (TK == kLogistic) {
         // the last probe of the sweep; the earlier ones are in lg_acc
         const bool multi = P.probes > 1;
         column_logistic<Real, QPL>(P, key, sm.Xs + c * Dp, t, iter, P.probes - 1,
@@ -776,22 +838,30 @@ static SweepKernels pick1(int tk, int jac, int qpl) {
                           : pick2<Real, kDenseGauss, kJacDiag>(qpl);
 }
 
-template <typename Real, int QPL>
+template <typename Real, int QPL, int JAC>
 static SweepKernels pick_logistic() {
   SweepKernels k;
-  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL, false>);
-  k.sweep_coop = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, kJacStoch, QPL, true>);
+  k.sweep = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, JAC, QPL, false>);
+  k.sweep_coop = reinterpret_cast<const void*>(&deer_sweep_kernel<Real, kLogistic, JAC, QPL, true>);
   k.finalize = reinterpret_cast<const void*>(&deer_finalize_logistic_kernel<Real>);
   k.init = reinterpret_cast<const void*>(&deer_init_kernel<Real>);
   k.eval = reinterpret_cast<const void*>(&lg_probe_accum_kernel<Real, QPL>);
   return k;
 }
 
-SweepKernels logistic_sweep_kernels(bool f64, int64_t D) {
+template <typename Real, int JAC>
+static SweepKernels pick_logistic_q(int qpl) {
+  return qpl == 1 ? pick_logistic<Real, 1, JAC>()
+                  : (qpl == 2 ? pick_logistic<Real, 2, JAC>() : pick_logistic<Real, 4, JAC>());
+}
+
+SweepKernels logistic_sweep_kernels(bool f64, int64_t D, int jac) {
   const int qpl = D <= 128 ? 1 : (D <= 256 ? 2 : 4);
   SweepKernels k;
-  if (f64) k = qpl == 1 ? pick_logistic<double, 1>() : (qpl == 2 ? pick_logistic<double, 2>() : pick_logistic<double, 4>());
-  else k = qpl == 1 ? pick_logistic<float, 1>() : (qpl == 2 ? pick_logistic<float, 2>() : pick_logistic<float, 4>());
+  if (jac == kJacDiag)
+    k = f64 ? pick_logistic_q<double, kJacDiag>(qpl) : pick_logistic_q<float, kJacDiag>(qpl);
+  else
+    k = f64 ? pick_logistic_q<double, kJacStoch>(qpl) : pick_logistic_q<float, kJacStoch>(qpl);
   k.qpl = qpl;
   return k;
 }

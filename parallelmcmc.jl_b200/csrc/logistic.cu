@@ -24,12 +24,20 @@ namespace pmcmc {
 // ---------------------------------------------------------------------------
 // Elementwise kernels
 // ---------------------------------------------------------------------------
+// Pass modes without tangent columns in the first GEMM, and modes evaluated at y.
+__host__ __device__ inline bool lg_value_only(int mode) { return mode == 2 || mode == 3 || mode == 4; }
+__host__ __device__ inline bool lg_at_y(int mode) { return mode == 1 || mode == 4 || mode == 5; }
 
 // B (Dp x ncols, column-major) for a column chunk [t0, t0+Tc):
 //   mode 0: [x_bar_t | z_t]   (x_bar_t = S_{t-1}, or x0 at t = 0 / first sweep; z_t the
 //                              Rademacher probe `probe` of this sweep)
 //   mode 1: [y_t | w_t]
 //   mode 2: [S_t]             (logp of the returned trajectory)
+// and, for the exact diagonal (:diag, see lg_mid_kernel):
+//   mode 3: [x_bar_t]         (the tangent half is filled by the epilogue)
+//   mode 4: [y_t]
+//   mode 5: [y_t | r_t],  r = x_bar - y - eps g_y
+//   mode 6: [x_bar_t | u_t], u from lg_acc
 // and zero the likelihood accumulators of the chunk.
 template <typename Real>
 __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
@@ -41,18 +49,30 @@ __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
   const bool from_x0 = iter == 0;
   const Real* S = static_cast<const Real*>(P.S[cur]);
   const Real* x0 = static_cast<const Real*>(P.x0);
-  const int ncols = mode == 2 ? Tc : 2 * Tc;
+  const int ncols = lg_value_only(mode) ? Tc : 2 * Tc;
   const int64_t n = static_cast<int64_t>(ncols) * Dp;
   const TapeKey key(P.seed, P.block);
+  const Real eps = static_cast<Real>(P.eps);
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int j = static_cast<int>(i / Dp);
     const int64_t d = i % Dp;
-    const bool tangent = j >= Tc && mode != 2;
+    const bool tangent = j >= Tc && !lg_value_only(mode);
     const int64_t t = t0 + (tangent ? j - Tc : j);
     Real v = Real(0);
     if (d < D && t < P.T) {
-      if (mode == 0) {
+      const Real* xb = (from_x0 || t == 0) ? x0 : S + (t - 1) * Dp;
+      if (mode >= 3) {
+        const Real* lg1 = static_cast<const Real*>(P.lg[1]);
+        if (mode == 3) v = xb[d];
+        else if (mode == 4) v = lg1[t * Dp + d];
+        else if (mode == 5)
+          v = tangent ? xb[d] - lg1[t * Dp + d] -
+                            eps * static_cast<const Real*>(P.lg[3])[t * Dp + d]
+                      : lg1[t * Dp + d];
+        else
+          v = tangent ? static_cast<const Real*>(P.lg_acc)[t * Dp + d] : xb[d];
+      } else if (mode == 0) {
         if (!tangent) {
           v = (from_x0 || t == 0) ? x0[d] : S[(t - 1) * Dp + d];
         } else {
@@ -69,7 +89,7 @@ __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
     }
     B[i] = v;
   }
-  double* lp = mode == 1 ? P.lpy : P.lpx;
+  double* lp = lg_at_y(mode) ? P.lpy : P.lpx;
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < Tc;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x)
     if (t0 + j < P.T) lp[t0 + j] = 0.0;
@@ -77,7 +97,9 @@ __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
 
 // Epilogue of a pass on the chunk intermediate L (N x ncols, column-major):
 // value column t -> r = y - sigmoid(l) with loglik = y l - softplus(l) summed
-// into lp[t] (FP64); tangent column -> s = sigmoid'(l) v.
+// into lp[t] (FP64); tangent column -> s = sigmoid'(l) v (has_tangent = 1), or
+// the weight sigmoid'(l) itself (has_tangent = 2: the diagonal of the Hessian,
+// contracted with X .* X).
 template <typename Real>
 __global__ void lg_epilogue_kernel(const Real* __restrict__ ylab, int64_t N, int Tc,
                                    int has_tangent, Real* __restrict__ L, double* __restrict__ lp,
@@ -96,7 +118,8 @@ __global__ void lg_epilogue_kernel(const Real* __restrict__ ylab, int64_t N, int
     const Real yn = ylab[n];
     acc += static_cast<double>(yn * l - sp);
     lv[n] = yn - p;
-    if (has_tangent) lt[n] = p * (Real(1) - p) * lt[n];
+    if (has_tangent == 1) lt[n] = p * (Real(1) - p) * lt[n];
+    else if (has_tangent == 2) lt[n] = p * (Real(1) - p);
   }
   acc = warp_sum(acc);
   __shared__ double red[32];
@@ -113,6 +136,19 @@ __global__ void lg_epilogue_kernel(const Real* __restrict__ ylab, int64_t N, int
 // y = x + eps g_x + sqrt(2 eps) xi, w = z + eps H(x) z;
 // stage 2 -> g_y = X'r - tau y, H(y) w = -X's - tau w.
 // G is Dp x 2Tc column-major (value block then tangent block).
+//
+// The exact diagonal of the surrogate Jacobian (:diag; the diagonal that
+// jac_diag_via_jvps, DEER.jl:327-342, gathers from D JVPs of MALA.jl:732-797)
+// is, with a the accept decision, g' the slope of the accept weight and
+// r = x_bar - y - eps g_y,
+//   J_ii = a (1 + eps H_x,ii) + (1 - a) + (y - x_bar)_i g' dla_i,
+//   dla = (g_y - g_x) + H_y r / 2 + H_x (eps g_y + r / 2 + eps H_y r / 2),
+// from four passes (modes 3-6) and these stages:
+//   stage 3 -> g_x, y, diag H_x = -(X.*X)'w - tau       into lg[0], lg[1], lg[2];
+//   stage 4 -> g_y                                      into lg[3];
+//   stage 5 -> v = H_y r: u = eps g_y + r/2 + eps v/2   into lg_acc,
+//              dla = g_y - g_x + v/2 so far              into lg[4];
+//   stage 6 -> dla += H_x u                              in lg[4].
 template <typename Real>
 __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* __restrict__ st,
                               int stage, int64_t t0, int Tc, int probe, const Real* __restrict__ G) {
@@ -165,7 +201,7 @@ __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* 
         static_cast<Real*>(P.lg[1])[o + e] = y;
         static_cast<Real*>(P.lg[2])[o + e] = w;
       }
-    } else {
+    } else if (stage == 2) {
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int64_t d = 4 * q + e;
@@ -178,6 +214,45 @@ __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* 
         }
         static_cast<Real*>(P.lg[3])[o + e] = gy;
         static_cast<Real*>(P.lg[4])[o + e] = hvy;
+      }
+    } else {
+      Real* lg0 = static_cast<Real*>(P.lg[0]);
+      Real* lg1 = static_cast<Real*>(P.lg[1]);
+      Real* lg2 = static_cast<Real*>(P.lg[2]);
+      Real* lg3 = static_cast<Real*>(P.lg[3]);
+      Real* lg4 = static_cast<Real*>(P.lg[4]);
+      Real* uacc = static_cast<Real*>(P.lg_acc);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t d = 4 * q + e;
+        const bool in = d < D;
+        const Real x = in ? ((from_x0 || t == 0) ? x0[d] : S[(t - 1) * Dp + d]) : Real(0);
+        if (stage == 3) {
+          Real gx = 0, y = 0, hd = 0;
+          if (in) {
+            gx = gv[e] - tau * x;
+            y = fma(c2, static_cast<Real>(P.xi[t * Dp + d]), fma(eps, gx, x));
+            hd = -gt[e] - tau;
+          }
+          lg0[o + e] = gx;
+          lg1[o + e] = y;
+          lg2[o + e] = hd;
+        } else if (stage == 4) {
+          lg3[o + e] = in ? gv[e] - tau * lg1[o + e] : Real(0);
+        } else if (stage == 5) {
+          Real u = 0, dl = 0;
+          if (in) {
+            const Real y = lg1[o + e], gy = lg3[o + e];
+            const Real r = x - y - eps * gy;
+            const Real v = -gt[e] - tau * r;
+            u = eps * gy + Real(0.5) * r + Real(0.5) * eps * v;
+            dl = (gy - lg0[o + e]) + Real(0.5) * v;
+          }
+          uacc[o + e] = u;
+          lg4[o + e] = dl;
+        } else {
+          if (in) lg4[o + e] += -gt[e] - tau * uacc[o + e];
+        }
       }
     }
   }
@@ -234,54 +309,92 @@ cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState
 }
 
 // One plain pass over all column chunks: prep -> L = X B -> epilogue -> G = X' L -> mid.
-// mode 0/1 = pass 1/2 (mid stage 1/2), mode 2 = logp pass (no tangent, no mid).
+// mode 0/1 = pass 1/2 (mid stage 1/2), mode 2 = logp pass (no tangent, no mid),
+// modes 3-6 = the passes of the exact diagonal (mid stages 3-6; mode 3 contracts
+// the weights of its tangent half with X2 = X .* X).
 int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
                   const DevParams* dP, const DevState* dS, double* lp, int mode, int64_t T,
                   int64_t Dp, void* Bbuf, void* Lbuf, void* Gbuf, int64_t Tc, int probe) {
   const int64_t N = X.N;
-  for (int64_t t0 = 0; t0 < T; t0 += Tc) {
-    const int tc = static_cast<int>(Tc);
-    const int ncols = mode == 2 ? tc : 2 * tc;
-    if (lg_prep(s, f64, dP, dS, mode, t0, tc, probe, Dp, Bbuf) != cudaSuccess) return 3;
+  const int n = static_cast<int>(N), dp = static_cast<int>(Dp);
+  // G = op(A) B for the column block [c0, c0 + nc) of L and G (A = X, or X2)
+  auto gemm = [&](bool first, const void* A, int c0, int nc) -> bool {
+    const size_t es = f64 ? 8 : 4;
+    const unsigned char* Bp = static_cast<const unsigned char*>(Bbuf) + es * c0 * Dp;
+    unsigned char* Lp = static_cast<unsigned char*>(Lbuf) + es * c0 * N;
+    unsigned char* Gp = static_cast<unsigned char*>(Gbuf) + es * c0 * Dp;
     cublasStatus_t st;
     if (f64) {
       const double one = 1.0, zero = 0.0;
-      st = cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(N), ncols,
-                       static_cast<int>(Dp), &one, static_cast<const double*>(X.X64),
-                       static_cast<int>(Dp), static_cast<const double*>(Bbuf),
-                       static_cast<int>(Dp), &zero, static_cast<double*>(Lbuf),
-                       static_cast<int>(N));
+      st = first ? cublasDgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, n, nc, dp, &one,
+                               static_cast<const double*>(A), dp,
+                               reinterpret_cast<const double*>(Bp), dp, &zero,
+                               reinterpret_cast<double*>(Lp), n)
+                 : cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, dp, nc, n, &one,
+                               static_cast<const double*>(A), dp,
+                               reinterpret_cast<const double*>(Lp), n, &zero,
+                               reinterpret_cast<double*>(Gp), dp);
     } else {
       const float one = 1.f, zero = 0.f;
-      st = cublasSgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(N), ncols,
-                       static_cast<int>(Dp), &one, X.X32, static_cast<int>(Dp),
-                       static_cast<const float*>(Bbuf), static_cast<int>(Dp), &zero,
-                       static_cast<float*>(Lbuf), static_cast<int>(N));
+      st = first ? cublasSgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, n, nc, dp, &one,
+                               static_cast<const float*>(A), dp,
+                               reinterpret_cast<const float*>(Bp), dp, &zero,
+                               reinterpret_cast<float*>(Lp), n)
+                 : cublasSgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, dp, nc, n, &one,
+                               static_cast<const float*>(A), dp,
+                               reinterpret_cast<const float*>(Lp), n, &zero,
+                               reinterpret_cast<float*>(Gp), dp);
     }
-    if (st != CUBLAS_STATUS_SUCCESS) return 3;
+    return st == CUBLAS_STATUS_SUCCESS;
+  };
+  const void* Xa = f64 ? static_cast<const void*>(X.X64) : static_cast<const void*>(X.X32);
+  const void* X2 = f64 ? static_cast<const void*>(X.X2_64) : static_cast<const void*>(X.X2_32);
+  if (mode == 3 && !X2) return 3;
+  for (int64_t t0 = 0; t0 < T; t0 += Tc) {
+    const int tc = static_cast<int>(Tc);
+    const bool vo = lg_value_only(mode);
+    if (lg_prep(s, f64, dP, dS, mode, t0, tc, probe, Dp, Bbuf) != cudaSuccess) return 3;
+    if (!gemm(true, Xa, 0, vo ? tc : 2 * tc)) return 3;
     const int64_t tmax = T - t0 < Tc ? T - t0 : Tc;
+    const int tang = mode == 3 ? 2 : (vo ? 0 : 1);
     if (lg_epilogue(s, f64, f64 ? static_cast<const void*>(X.y64) : static_cast<const void*>(X.y32),
-                    N, tc, mode != 2, Lbuf, lp + t0, tmax) != cudaSuccess)
+                    N, tc, tang, Lbuf, lp + t0, tmax) != cudaSuccess)
       return 3;
     if (mode == 2) continue;
-    if (f64) {
-      const double one = 1.0, zero = 0.0;
-      st = cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, static_cast<int>(Dp), ncols,
-                       static_cast<int>(N), &one, static_cast<const double*>(X.X64),
-                       static_cast<int>(Dp), static_cast<const double*>(Lbuf),
-                       static_cast<int>(N), &zero, static_cast<double*>(Gbuf),
-                       static_cast<int>(Dp));
-    } else {
-      const float one = 1.f, zero = 0.f;
-      st = cublasSgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, static_cast<int>(Dp), ncols,
-                       static_cast<int>(N), &one, X.X32, static_cast<int>(Dp),
-                       static_cast<const float*>(Lbuf), static_cast<int>(N), &zero,
-                       static_cast<float*>(Gbuf), static_cast<int>(Dp));
+    if (mode == 3) {
+      if (!gemm(false, Xa, 0, tc) || !gemm(false, X2, tc, tc)) return 3;
+    } else if (!gemm(false, Xa, 0, vo ? tc : 2 * tc)) {
+      return 3;
     }
-    if (st != CUBLAS_STATUS_SUCCESS) return 3;
-    if (lg_mid(s, f64, dP, dS, mode + 1, t0, tc, probe, Dp, Gbuf) != cudaSuccess) return 3;
+    const int stage = mode <= 1 ? mode + 1 : mode;
+    if (lg_mid(s, f64, dP, dS, stage, t0, tc, probe, Dp, Gbuf) != cudaSuccess) return 3;
   }
   return 0;
+}
+
+// X2 = X .* X (the rows and padding of X), for the diagonal of the Hessian.
+template <typename Real>
+__global__ void lg_square_kernel(const Real* __restrict__ X, Real* __restrict__ X2, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    X2[i] = X[i] * X[i];
+}
+
+cudaError_t lg_make_square(cudaStream_t s, LogisticDev& X, bool f64) {
+  const int64_t n = X.N * X.Dp;
+  const int g = grid_for(n);
+  if (f64) {
+    if (X.X2_64) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&X.X2_64, 8 * n);
+    if (e != cudaSuccess) return e;
+    lg_square_kernel<double><<<g, 256, 0, s>>>(X.X64, X.X2_64, n);
+  } else {
+    if (X.X2_32) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&X.X2_32, 4 * n);
+    if (e != cudaSuccess) return e;
+    lg_square_kernel<float><<<g, 256, 0, s>>>(X.X32, X.X2_32, n);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace pmcmc

@@ -24,6 +24,9 @@ struct LogisticDev {
   int64_t Np = 0, Dk = 0;
   __half* Xh = nullptr;
   __half* Xl = nullptr;
+  // X .* X for the exact diagonal (:diag), made on first use (lg_make_square)
+  float* X2_32 = nullptr;
+  double* X2_64 = nullptr;
 };
 
 int64_t lg_chunk_cols(int64_t N, int64_t T);
@@ -34,6 +37,8 @@ int lg_plain_pass(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool 
 
 cudaError_t lg_mid(cudaStream_t s, bool f64, const DevParams* dP, const DevState* dS, int stage,
                    int64_t t0, int Tc, int probe, int64_t Dp, const void* G);
+// X2 = X .* X in the state's precision (once; the caller serialises first uses).
+cudaError_t lg_make_square(cudaStream_t s, LogisticDev& X, bool f64);
 
 // Tensor-core pass (logistic_tc.cu): mode 0/1/2 as in lg_plain_pass; writes G
 // (Dp x 2T FP32, value block then tangent block) and lp.  ws holds the FP16

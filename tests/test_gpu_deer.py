@@ -553,9 +553,33 @@ def test_logistic_probes_on_tensor_cores_match_sequential(h):
     assert trace_err(S, S_seq) <= 1e-5
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_logistic_exact_diagonal(h, dtype):
+    # :diag on the logistic target: the diagonal jac_diag_via_jvps (DEER.jl:327-342)
+    # gathers from D JVPs, here in closed form from four contraction passes.  FP64 takes
+    # the oracle's iterates (D JVPs a column); FP32 meets the sequential chain.
+    N, D, T, eps = 220, 9, 80, 0.03
+    X, y = _logistic_problem(N, D, 37)
+    model = pmcmc.DensityModel.logistic(X, y)
+    tight = {} if dtype == np.float64 else dict(tol_abs=1e-7, tol_rel=1e-6)
+    sampler = pmcmc.ParallelMALASampler(eps, T=T, jacobian="diag", dtype=dtype, **tight)
+    S, info, lp, acc = _run(h, model, sampler, np.zeros(D, dtype), 14, 0)
+    tg = O.Target.logistic(X, y)
+    Xi, u = O.tape(14, 0, D, T)
+    assert info["converged"], info
+    if dtype == np.float64:
+        S_cpu, icpu = O.deer_solve(tg, eps, np.zeros(D), Xi, u, 14, 0, jacobian="diag")
+        assert info["iters"] == icpu["iters"]
+        np.testing.assert_allclose(S, S_cpu, rtol=1e-9, atol=1e-10)
+    S_seq, acc_seq, _ = O.mala_sequential(tg, eps, np.zeros(D), Xi, u)
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= (1e-5 if dtype == np.float32 else 5e-5)
+
+
 def test_logistic_unsupported_modes(h):
     X, y = _logistic_problem(50, 4, 33)
     model = pmcmc.DensityModel.logistic(X, y)
     with pytest.raises(pmcmc.Unsupported):
-        pmcmc.solve(model, pmcmc.ParallelMALASampler(0.01, T=16, jacobian="diag"), np.zeros(4),
+        pmcmc.solve(model, pmcmc.ParallelMALASampler(0.01, T=16, jacobian="full",
+                                                     dtype=np.float32), np.zeros(4, np.float32),
                     handle=h)
