@@ -52,6 +52,8 @@ struct SliceState {
       out_acc, x_next, total;
 };
 
+constexpr size_t kCublasWsBytes = size_t(32) << 20;
+
 struct pmcmc_handle {
   int device = 0;
   int num_sms = 148;
@@ -89,6 +91,7 @@ struct pmcmc_handle {
   int tune_per_sm = 0;
   int tune_full_chunks = 0;
   SliceState slice;
+  void* cublas_ws = nullptr;  // cuBLAS workspace of its own (no allocation inside its calls)
   std::vector<pmcmc_handle*> fleet;  // worker handles of pmcmc_fleet_solve (own streams)
   // host-output pipeline of multi-block solves: block b's device-to-host copy
   // runs on copy_stream while block b + 1 solves on stream
@@ -717,6 +720,7 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   const TieBufs tb = lg_tie_carve(ws + L.tie, tg->lg, P.T, tie_kmax(P.T));
   P.la_ref = refine ? la_ref : nullptr;
   P.lg_acc = ws + L.lg_acc;
+  P.tc_err = use_tc ? lg_tc_err_word(ws + L.tcws, tg->lg, P.T) : nullptr;
   const void* k_acc = k.eval;  // the probe accumulation kernel of the logistic target
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 0)
@@ -725,6 +729,10 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
       return fail(h, PMCMC_ERR_CUDA, "cublasCreate failed");
     cublasSetMathMode(h->cublas, CUBLAS_PEDANTIC_MATH);
+    // a workspace of its own: cuBLAS then allocates nothing during the solve
+    CK(cudaMalloc(&h->cublas_ws, kCublasWsBytes));
+    if (cublasSetWorkspace(h->cublas, h->cublas_ws, kCublasWsBytes) != CUBLAS_STATUS_SUCCESS)
+      return fail(h, PMCMC_ERR_CUDA, "cublasSetWorkspace failed");
   }
   cublasSetStream(h->cublas, h->stream);
   void* init_args[] = {&h->d_params, &h->d_state};
@@ -780,7 +788,8 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   const int grid_acc = static_cast<int>(std::min<int64_t>((P.T + kWarps - 1) / kWarps,
                                                           int64_t(h->num_sms) * 8));
   const bool lg_diag = P.jac == PMCMC_JAC_DIAG;
-  for (int it = 0; it < P.maxiter; ++it) {
+  // The launches of one Newton sweep, ending with the finish-and-scan kernel.
+  auto issue_sweep = [&]() -> int {
     // exact diagonal: g_x, y, diag H_x | g_y | H_y r | H_x u (logistic.cu, modes 3-6)
     for (int m = 3; lg_diag && m <= 6; ++m) {
       if (pass(m, m == 4 || m == 5 ? P.lpy : P.lpx))
@@ -803,7 +812,8 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
         if (rc) return rc;
       }
       if (pr + 1 < P.probes) {
-        void* acc_args[] = {&h->d_params, &h->d_state, &pr};
+        int probe = pr;
+        void* acc_args[] = {&h->d_params, &h->d_state, &probe};
         CK(cudaLaunchKernel(k_acc, dim3(grid_acc), dim3(kThreads), acc_args, 0, h->stream));
       }
     }
@@ -811,6 +821,13 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
     CK(launch_sweep(coop ? k.sweep_coop : k.sweep, coop, P.ntiles, smem_sweep, sweep_args,
                     h->stream));
     if (h->profiling) CK(cudaEventRecord(h->ev[1], h->stream));
+    return PMCMC_OK;
+  };
+  // The Newton loop: one sweep after another, with a host check of the state after
+  // each (the convergence test, maxiter, a non-finite state, a tensor-core wait error).
+  auto eager_sweep = [&]() -> int {  // one sweep with the host check of its state
+    const int rc = issue_sweep();
+    if (rc) return rc;
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
                        h->stream));
     if (use_tc)
@@ -823,6 +840,11 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
       h->prof.sweep_ms += ms;
     }
     if (*h_err) return fail(h, PMCMC_ERR_TIMEOUT, "tensor-core pass: a bounded wait gave up");
+    return PMCMC_OK;
+  };
+  for (int it = 0; it < P.maxiter; ++it) {
+    const int rc = eager_sweep();
+    if (rc) return rc;
     if (h->h_state->converged || h->h_state->status) break;
   }
   if (!plain && !h->h_state->status) {
@@ -1621,6 +1643,7 @@ int pmcmc_destroy(pmcmc_handle* h) {
   }
   if (h->h_states) cudaFreeHost(h->h_states);
   if (h->cublas) cublasDestroy(h->cublas);
+  cudaFree(h->cublas_ws);
   cudaFree(h->d_full);
   cudaFree(h->d_params_e);
   cudaFree(h->ws);

@@ -63,6 +63,8 @@ struct DevParams {
   const double* la_ref;
   // probes > 1: sum of z_k .* J z_k over the probes 0 .. probes-2 of the sweep (T x Dp, Real)
   void* lg_acc;
+  // error word of the tensor-core pass (a bounded wait gave up), or nullptr
+  const int* tc_err;
   double tau;  // prior precision
   // tape of the block, written once by the init kernel: xi (T x Dp, FP32,
   // padded rows zero) and log(u_t) in FP64

@@ -493,6 +493,9 @@ __global__ void __launch_bounds__(kThreads)
     new_t_lo = s_first;
   }
   if (tid == 0) {
+    // a tensor-core pass of this sweep gave up a wait: its results are not to be used
+    if (P.tc_err && *reinterpret_cast<const volatile int*>(P.tc_err))
+      atomicCAS(&st->status, 0, static_cast<int>(kStTimeout));
     const int status = atomicAdd(&st->status, 0);
     const int converged = windowed ? (new_t_lo >= T) : (metric <= 1.0);
     st->metric = metric;
