@@ -130,6 +130,21 @@ int pmcmc_target_dense_gauss(pmcmc_handle* h, int64_t D, const double* mean,
                              const double* prec, pmcmc_target** out);
 int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X,
                           const double* y, double prior_prec, pmcmc_target** out);
+/* Mass matrix M = L L^T: replaces the `cholM = cholesky(M)` keyword of
+ * MALASampler / ParallelMALASampler / AdaptiveMALASampler (src/interface.jl:
+ * 84-100, 241-287, 899-930) that MALA.jl applies in every step (src/MALA/MALA.jl:
+ * 29-47).  `L` is the D x D lower Cholesky factor, column-major host memory
+ * (entries above the diagonal are ignored; the diagonal must be positive).
+ * Returns a new target, independent of `base` (which may be destroyed), whose
+ * solves, samples and sequential chains (pmcmc_deer_solve, pmcmc_sample,
+ * pmcmc_fleet_solve, pmcmc_mala_chains) run the chain with mass M, outputs in
+ * the base target's coordinates; internally it is the whitened Gaussian
+ * x' = L^-1 x (precision L^T P L, mean L^-1 mean), where the same tape gives the
+ * same chain, and its `info` defects are in those coordinates.  Gaussian bases
+ * with D <= 4096; logistic bases, the adjoint and slices return
+ * PMCMC_ERR_UNSUPPORTED. */
+int pmcmc_target_mass(pmcmc_handle* h, const pmcmc_target* base, const double* L,
+                      pmcmc_target** out);
 int pmcmc_target_destroy(pmcmc_target* t);
 
 /* ---- tape ------------------------------------------------------------------

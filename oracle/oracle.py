@@ -86,6 +86,8 @@ def lib():
                                     _dp, _ip]
         L.orc_mala_sequential.argtypes = [C.POINTER(_Target), C.c_double, _dp, _dp, _dp,
                                           C.c_int64, _dp, _ip, _dp]
+        L.orc_mala_sequential_mass.argtypes = [C.POINTER(_Target), C.c_double, _dp, _dp, _dp,
+                                               _dp, C.c_int64, _dp, _ip, _dp]
         L.orc_mala_sequential_logistic.argtypes = [C.POINTER(_Target), C.c_double, _dp, _dp,
                                                    _dp, C.c_int64, _dp, _ip, _dp, C.c_int32]
         L.orc_fwd_and_jvp.argtypes = [C.POINTER(_Target), C.c_double, _dp, _dp, C.c_double,
@@ -221,6 +223,22 @@ def mala_sequential(tg, eps, x0, Xi, u):
     la = np.empty(T)
     lib().orc_mala_sequential(tg.ref(), eps, _p(x0), _p(Xi_c), _p(u), T, _p(S),
                               _p(acc, _ip), _p(la))
+    return S.T, acc.astype(bool), la
+
+
+def mala_sequential_mass(tg, eps, Lfac, x0, Xi, u):
+    """Sequential MALA with mass matrix M = L L^T (L lower triangular): returns
+    S (D, T), accepted (T,), logalpha (T,)."""
+    Xi_c = _col(Xi)
+    T, D = Xi_c.shape
+    Lc = np.ascontiguousarray(np.asarray(Lfac, np.float64).T)  # column-major
+    u = np.ascontiguousarray(u, np.float64)
+    x0 = np.ascontiguousarray(x0, np.float64)
+    S = np.empty((T, D))
+    acc = np.empty(T, np.int32)
+    la = np.empty(T)
+    lib().orc_mala_sequential_mass(tg.ref(), eps, _p(Lc), _p(x0), _p(Xi_c), _p(u), T, _p(S),
+                                   _p(acc, _ip), _p(la))
     return S.T, acc.astype(bool), la
 
 

@@ -424,6 +424,69 @@ void orc_mala_sequential_logistic(const orc_target* tg, double eps, const double
     free(buf);
 }
 
+/* Mass-matrix MALA with M = L L^T (cholM of the reference), L lower triangular,
+ * D x D column-major: _apply_M! (MALA.jl:29-35), _apply_L! (:37-38), _quad_Minv!
+ * (:40-44), _logdet_M (:46-47), the proposal (:207-229), logq_mala! (:160-193) and
+ * the strict accept test of mala_step_with_logalpha! (:377-411).  S column t = x_{t+1}. */
+static void lower_mv(int64_t D, const double* L, const double* v, double* out) {
+    for (int64_t i = 0; i < D; ++i) out[i] = 0.0;
+    for (int64_t k = 0; k < D; ++k)
+        for (int64_t i = k; i < D; ++i) out[i] += L[k * D + i] * v[k];
+}
+static void lower_t_mv(int64_t D, const double* L, const double* v, double* out) {
+    for (int64_t k = 0; k < D; ++k) {
+        double s = 0.0;
+        for (int64_t i = k; i < D; ++i) s += L[k * D + i] * v[i];
+        out[k] = s;
+    }
+}
+/* |L^-1 r|^2 by forward substitution (ldiv! with the lower factor) */
+static double quad_minv(int64_t D, const double* L, const double* r, double* tmp) {
+    double q = 0.0;
+    for (int64_t i = 0; i < D; ++i) {
+        double s = r[i];
+        for (int64_t k = 0; k < i; ++k) s -= L[k * D + i] * tmp[k];
+        tmp[i] = s / L[i * D + i];
+        q += tmp[i] * tmp[i];
+    }
+    return q;
+}
+
+void orc_mala_sequential_mass(const orc_target* tg, double eps, const double* L, const double* x0,
+                              const double* Xi, const double* u, int64_t T, double* S,
+                              int32_t* accepted, double* logalpha) {
+    const int64_t D = tg->D;
+    double* b = (double*)malloc(sizeof(double) * 9 * D);
+    double *x = b, *gx = b + D, *y = b + 2 * D, *gy = b + 3 * D, *mg = b + 4 * D,
+           *lx = b + 5 * D, *tmp = b + 6 * D, *r = b + 7 * D, *t2 = b + 8 * D;
+    double logdet = 0.0;
+    for (int64_t i = 0; i < D; ++i) logdet += 2.0 * log(L[i * D + i]);
+    const double c = (double)D / 2 * log(4 * M_PI * eps);
+    const double s2e = sqrt(2 * eps);
+    memcpy(x, x0, sizeof(double) * D);
+    for (int64_t t = 0; t < T; ++t) {
+        orc_grad(tg, x, gx);
+        lower_t_mv(D, L, gx, tmp);
+        lower_mv(D, L, tmp, mg);           /* M g_x */
+        lower_mv(D, L, Xi + t * D, lx);    /* L xi */
+        for (int64_t i = 0; i < D; ++i) y[i] = x[i] + eps * mg[i] + s2e * lx[i];
+        orc_grad(tg, y, gy);
+        for (int64_t i = 0; i < D; ++i) r[i] = y[i] - (x[i] + eps * mg[i]);
+        const double lq_yx = -0.5 * quad_minv(D, L, r, t2) / (2 * eps) - c - 0.5 * logdet;
+        lower_t_mv(D, L, gy, tmp);
+        lower_mv(D, L, tmp, mg);           /* M g_y */
+        for (int64_t i = 0; i < D; ++i) r[i] = x[i] - (y[i] + eps * mg[i]);
+        const double lq_xy = -0.5 * quad_minv(D, L, r, t2) / (2 * eps) - c - 0.5 * logdet;
+        const double la = (orc_logp(tg, y) + lq_xy) - (orc_logp(tg, x) + lq_yx);
+        const int acc = log(u[t]) < la;
+        if (acc) memcpy(x, y, sizeof(double) * D);
+        memcpy(S + t * D, x, sizeof(double) * D);
+        if (accepted) accepted[t] = acc;
+        if (logalpha) logalpha[t] = la;
+    }
+    free(b);
+}
+
 /* Per-column fused forward + surrogate JVP in the batched operation order of
  * mala_step_batched_fwd_and_jvp! (MALA.jl:577-626), identity mass matrix. */
 static void fwd_jvp_col(const orc_target* tg, double eps, const double* x, const double* xi,

@@ -88,6 +88,10 @@ void orc_mala_sequential(const orc_target* tg, double eps, const double* x0, con
 void orc_mala_sequential_logistic(const orc_target* tg, double eps, const double* x0,
                                   const double* Xi, const double* u, int64_t T, double* S,
                                   int32_t* accepted, double* logalpha, int32_t nthreads);
+/* Sequential MALA with mass matrix M = L L^T (L lower triangular, D x D column-major). */
+void orc_mala_sequential_mass(const orc_target* tg, double eps, const double* L, const double* x0,
+                              const double* Xi, const double* u, int64_t T, double* S,
+                              int32_t* accepted, double* logalpha);
 void orc_fwd_and_jvp(const orc_target* tg, double eps, const double* x, const double* xi,
                      double u, const double* v, double* f, double* jv);
 void orc_fwd_and_jvp_batched(const orc_target* tg, double eps, int64_t T, const double* X,

@@ -127,6 +127,11 @@ struct pmcmc_target {
   double* zq_d = nullptr;    // Dq zeros
   float* qrmq = nullptr;     // Dq x Dq, Q row-major
   float* qcmq = nullptr;     // Dq x Dq, Q column-major
+  std::vector<double> mean_host;  // D (Gaussian targets)
+  // Mass-matrix targets (pmcmc_target_mass): this target is the whitened one,
+  // and L (D x D column-major, lower triangular) maps its chains back.
+  std::vector<double> mass_L;
+  double* mass_Ld = nullptr;
 };
 
 namespace {
@@ -1214,9 +1219,9 @@ int status_error(pmcmc_handle* h, int status) {
 
 // Shared implementation of pmcmc_deer_solve (nblocks = 1, N = T) and
 // pmcmc_sample (block loop of interface.jl:584-599).
-int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
-                 const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
-                 void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
+int solve_core(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+               const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
+               void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
   int rc = validate(h, tg, p);
   if (rc) return rc;
   if (!x0 || !S_out) return fail(h, PMCMC_ERR_ARGUMENT, "x0 and the output must not be NULL");
@@ -1508,6 +1513,64 @@ int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_param
   return status_error(h, status);
 }
 
+// A mass-matrix target (M = L L^T, the reference's cholM) is stored as the
+// whitened Gaussian x' = L^-1 x.  MALA with mass M is plain MALA on the
+// whitened target with the same tape and the same log alpha (src/MALA/MALA.jl:
+// 29-47 applies L, L^T and L \ inside every step), so the Newton solve runs in
+// whitened coordinates: x0 is whitened once on the device, the solve writes to
+// device memory, every column maps back as S = L S' in place, and host outputs
+// are copied out last.  log p and the accept flags are coordinate-free; the
+// defects in `info` are in whitened coordinates.
+int solve_mass(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+               const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
+               void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0 || !S_out) return fail(h, PMCMC_ERR_ARGUMENT, "x0 and the output must not be NULL");
+  if (mem != PMCMC_MEM_HOST && mem != PMCMC_MEM_DEVICE)
+    return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
+  if (N < 1) return fail(h, PMCMC_ERR_ARGUMENT, "the number of samples must be >= 1");
+  DeviceGuard guard(h->device);
+  const bool f64 = p->dtype == PMCMC_F64;
+  const size_t es = f64 ? 8 : 4;
+  const int64_t D = tg->D;
+  const bool host = mem == PMCMC_MEM_HOST;
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t bx = up(es * D), bS = host ? up(es * N * D) : 0,
+               blp = host && logp_out ? up(es * N) : 0, bac = host && accept_out ? up(N) : 0;
+  struct Scratch {
+    void* buf = nullptr;
+    ~Scratch() { cudaFree(buf); }
+  } sc;
+  CK(cudaMalloc(&sc.buf, 2 * bx + bS + blp + bac));
+  unsigned char* b = static_cast<unsigned char*>(sc.buf);
+  CK(cudaMemcpyAsync(b, x0, es * D, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                     h->stream));
+  CK(mass_whiten(h->stream, tg->mass_Ld, D, 1, b, b + bx, f64));
+  void* S = host ? b + 2 * bx : S_out;
+  void* lp = host ? (logp_out ? b + 2 * bx + bS : nullptr) : logp_out;
+  uint8_t* ac = host ? (accept_out ? b + 2 * bx + bS + blp : nullptr) : accept_out;
+  rc = solve_core(h, tg, p, b + bx, seed, block0, N, S, lp, ac, PMCMC_MEM_DEVICE, info);
+  if (rc) return rc;
+  CK(mass_map(h->stream, tg->mass_Ld, D, N, S, f64, h->num_sms));
+  if (host) {
+    CK(cudaMemcpyAsync(S_out, S, es * N * D, cudaMemcpyDeviceToHost, h->stream));
+    if (logp_out) CK(cudaMemcpyAsync(logp_out, lp, es * N, cudaMemcpyDeviceToHost, h->stream));
+    if (accept_out)
+      CK(cudaMemcpyAsync(accept_out, ac, N, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PMCMC_OK;
+}
+
+int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                 const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
+                 void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
+  if (tg && tg->mass_Ld)
+    return solve_mass(h, tg, p, x0, seed, block0, N, S_out, logp_out, accept_out, mem, info);
+  return solve_core(h, tg, p, x0, seed, block0, N, S_out, logp_out, accept_out, mem, info);
+}
+
 int make_target(pmcmc_handle* h, int kind, int64_t D, const double* mean, const double* prec,
                 pmcmc_target** out) {
   if (!h) return PMCMC_ERR_ARGUMENT;
@@ -1533,6 +1596,7 @@ int make_target(pmcmc_handle* h, int kind, int64_t D, const double* mean, const 
   }
   std::vector<float> mf(md.begin(), md.end()), pf(pd.begin(), pd.end());
   t->prec_host.assign(prec, prec + (kind == kDenseGauss ? D * D : D));
+  t->mean_host.assign(md.begin(), md.begin() + D);
   auto cleanup = [&]() {
     cudaFree(t->mean_d);
     cudaFree(t->prec_d);
@@ -1726,6 +1790,81 @@ int pmcmc_target_dense_gauss(pmcmc_handle* h, int64_t D, const double* mean, con
   return make_target(h, kDenseGauss, D, mean, prec, out);
 }
 
+// The reference's cholM = cholesky(M) on MALASampler / ParallelMALASampler /
+// AdaptiveMALASampler (src/interface.jl:84-100, 241-287, 899-930), applied by
+// MALA.jl's _apply_M!, _apply_L!, _quad_Minv! and _logdet_M (src/MALA/MALA.jl:
+// 29-47).  The new target is the base Gaussian in whitened coordinates
+// x' = L^-1 x: precision L^T P L, mean L^-1 mu; it keeps L to map chains back.
+int pmcmc_target_mass(pmcmc_handle* h, const pmcmc_target* base, const double* L,
+                      pmcmc_target** out) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  if (!out) return fail(h, PMCMC_ERR_ARGUMENT, "out must not be NULL");
+  if (!base || !L) return fail(h, PMCMC_ERR_ARGUMENT, "base target and L must not be NULL");
+  if (base->kind == kLogistic)
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "mass matrix: built for Gaussian targets");
+  if (base->mass_Ld)
+    return fail(h, PMCMC_ERR_ARGUMENT, "base target already carries a mass matrix");
+  const int64_t D = base->D;
+  if (D > mass_max_dim())
+    return fail(h, PMCMC_ERR_UNSUPPORTED, "mass matrix: built for D <= %lld",
+                (long long)mass_max_dim());
+  const size_t DD = static_cast<size_t>(D) * D;
+  std::vector<double> Lc(DD, 0.0);  // lower triangle only
+  for (int64_t j = 0; j < D; ++j) {
+    if (!(L[j * D + j] > 0) || !std::isfinite(L[j * D + j]))
+      return fail(h, PMCMC_ERR_ARGUMENT, "L must have a positive diagonal (L[%lld,%lld] = %g)",
+                  (long long)j, (long long)j, L[j * D + j]);
+    for (int64_t i = j; i < D; ++i) {
+      if (!std::isfinite(L[j * D + i]))
+        return fail(h, PMCMC_ERR_ARGUMENT, "L has a non-finite entry");
+      Lc[j * D + i] = L[j * D + i];
+    }
+  }
+  // P L (column j of L is zero above row j), then L^T (P L), symmetrised
+  const bool dense = base->kind == kDenseGauss;
+  const std::vector<double>& P = base->prec_host;
+  std::vector<double> PL(DD, 0.0), Pw(DD, 0.0);
+  for (int64_t j = 0; j < D; ++j)
+    for (int64_t k = j; k < D; ++k) {
+      const double l = Lc[j * D + k];
+      if (dense)
+        for (int64_t i = 0; i < D; ++i) PL[j * D + i] += P[k * D + i] * l;
+      else
+        PL[j * D + k] += P[k] * l;
+    }
+  for (int64_t j = 0; j < D; ++j)
+    for (int64_t i = 0; i <= j; ++i) {
+      double acc = 0.0;
+      for (int64_t k = i; k < D; ++k) acc += Lc[i * D + k] * PL[j * D + k];
+      Pw[j * D + i] = acc;
+    }
+  for (int64_t j = 0; j < D; ++j)
+    for (int64_t i = j + 1; i < D; ++i) Pw[j * D + i] = Pw[i * D + j];
+  // mu' = L^-1 mu (forward substitution)
+  std::vector<double> mw(static_cast<size_t>(D));
+  for (int64_t i = 0; i < D; ++i) {
+    double r = base->mean_host[i];
+    for (int64_t k = 0; k < i; ++k) r -= Lc[k * D + i] * mw[k];
+    mw[i] = r / Lc[i * D + i];
+  }
+  pmcmc_target* t = nullptr;
+  int rc = make_target(h, kDenseGauss, D, mw.data(), Pw.data(), &t);
+  if (rc) return rc;
+  DeviceGuard guard(h->device);
+  t->mass_L = std::move(Lc);
+  cudaError_t e = cudaMalloc(&t->mass_Ld, 8 * DD);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->mass_Ld, t->mass_L.data(), 8 * DD, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    pmcmc_target_destroy(t);
+    return fail(h, e == cudaErrorMemoryAllocation ? PMCMC_ERR_NOMEM : PMCMC_ERR_CUDA,
+                "mass matrix upload failed: %s", cudaGetErrorString(e));
+  }
+  *out = t;
+  return PMCMC_OK;
+}
+
 int pmcmc_target_logistic(pmcmc_handle* h, int64_t N, int64_t D, const double* X,
                           const double* y, double prior_prec, pmcmc_target** out) {
   if (!h) return PMCMC_ERR_ARGUMENT;
@@ -1813,6 +1952,7 @@ int pmcmc_target_destroy(pmcmc_target* t) {
   cudaFree(t->lg.Xl);
   cudaFree(t->lg.X2_32);
   cudaFree(t->lg.X2_64);
+  cudaFree(t->mass_Ld);
   for (void* q : {static_cast<void*>(t->lam_f), static_cast<void*>(t->qrm_f),
                   static_cast<void*>(t->qcm_f), static_cast<void*>(t->lamq_f),
                   static_cast<void*>(t->lamq_d), static_cast<void*>(t->zq_f),
@@ -2109,11 +2249,15 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
   uint8_t* dacc = accept_out;
   const size_t bx = es * n * D, bs = 8 * static_cast<size_t>(n), bS = es * n * T * D,
                blp = logp_out ? es * n * T : 0, bacc = accept_out ? n * T : 0;
+  // mass-matrix targets: the chains run whitened from x0' = L^-1 x0 (the
+  // solve's whitening, solve_mass), and map back in place after the launch
+  const bool mass = tg->mass_Ld != nullptr;
+  auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t bw = mass ? a(bx) : 0;
   if (mem == PMCMC_MEM_HOST) {
-    auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
-    rc = ensure_ws(h, a(bx) + a(bs) + a(bS) + a(blp) + a(bacc));
+    rc = ensure_ws(h, bw + a(bx) + a(bs) + a(bS) + a(blp) + a(bacc));
     if (rc) return rc;
-    unsigned char* w = h->ws;
+    unsigned char* w = h->ws + bw;
     dx0 = w;
     dseeds = reinterpret_cast<const uint64_t*>(w + a(bx));
     dS = w + a(bx) + a(bs);
@@ -2122,8 +2266,16 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
     CK(cudaMemcpyAsync(const_cast<void*>(dx0), x0, bx, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(const_cast<uint64_t*>(dseeds), seeds, bs, cudaMemcpyHostToDevice,
                        h->stream));
+  } else if (mass) {
+    rc = ensure_ws(h, bw);
+    if (rc) return rc;
+  }
+  if (mass) {
+    CK(mass_whiten(h->stream, tg->mass_Ld, D, n, dx0, h->ws, f64));
+    dx0 = h->ws;
   }
   CK(launch_mala_chains(h->stream, f64, tg->kind, P, n, dx0, dseeds, dS, dlp, dacc));
+  if (mass) CK(mass_map(h->stream, tg->mass_Ld, D, n * T, dS, f64, h->num_sms));
   if (mem == PMCMC_MEM_HOST) {
     CK(cudaMemcpyAsync(S_out, dS, bS, cudaMemcpyDeviceToHost, h->stream));
     if (logp_out) CK(cudaMemcpyAsync(logp_out, dlp, blp, cudaMemcpyDeviceToHost, h->stream));
@@ -2156,6 +2308,7 @@ int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer
     return fail(h, PMCMC_ERR_ARGUMENT, "objective must be PMCMC_OBJ_ESJD or PMCMC_OBJ_MEAN_SQ");
   if (tg->kind == kLogistic)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for the Gaussian targets");
+  if (tg->mass_Ld) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint takes no mass matrix");
   if (p->dtype != PMCMC_F32) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for FP32");
   const int64_t D = tg->D, Dp = tg->Dp, T = p->T;
   if (Dp > 128) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for D <= 128");
@@ -2295,6 +2448,7 @@ int pmcmc_slice_begin(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
   if (!x0) return fail(h, PMCMC_ERR_ARGUMENT, "x0 must not be NULL");
   if (tg->kind == kLogistic)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "slices are built for the Gaussian targets");
+  if (tg->mass_Ld) return fail(h, PMCMC_ERR_UNSUPPORTED, "slices take no mass matrix");
   if (p->jacobian == PMCMC_JAC_FULL)
     return fail(h, PMCMC_ERR_UNSUPPORTED, "slices take the diagonal Jacobians");
   if (t0 < 0 || W < 1 || t0 + W > p->T)

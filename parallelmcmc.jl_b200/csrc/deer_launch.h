@@ -85,4 +85,12 @@ cudaError_t launch_lookback_bound(cudaStream_t s, const uint32_t* flags, int* er
 cudaError_t launch_broadcast(cudaStream_t s, bool f64, int64_t Dp, int64_t T, const void* x0,
                              void* S);
 
+// Mass matrix M = L L^T (mass.cu), L column-major lower triangular in FP64:
+// y = L^-1 x for n D-vectors and S[:, j] <- L S[:, j] for N columns, in place.
+int64_t mass_max_dim();
+cudaError_t mass_whiten(cudaStream_t s, const double* L, int64_t D, int64_t n, const void* x,
+                        void* y, bool f64);
+cudaError_t mass_map(cudaStream_t s, const double* L, int64_t D, int64_t N, void* S, bool f64,
+                     int num_sms);
+
 }  // namespace pmcmc

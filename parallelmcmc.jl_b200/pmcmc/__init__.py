@@ -8,10 +8,10 @@ from types import SimpleNamespace
 from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupported,
                    default_handle, load)
 from .adapt import AdaptiveMALASampler, adapt_step_size, dual_average_update
-from .core import (Chain, DensityModel, ParallelMALASampler, ParallelMALAState,
+from .core import (Chain, Cholesky, DensityModel, ParallelMALASampler, ParallelMALAState,
                    ParallelMALATransition, adjoint, autotune, fleet_solve, mala_chains, sample,
                    solve,
-                   solve_affine_scan_diag, step, tape)
+                   cholesky, solve_affine_scan_diag, step, tape)
 
 # Module-style aliases matching ParallelMCMC.DEER / ParallelMCMC.DEERScan.
 DEER = SimpleNamespace(solve=solve, adjoint=adjoint, solve_affine_scan_diag=solve_affine_scan_diag)
@@ -22,5 +22,5 @@ __all__ = [
     "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
     "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
     "step", "tape", "mala_chains", "autotune", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
-    "solve_affine_scan_diag", "DEER", "DEERScan",
+    "solve_affine_scan_diag", "DEER", "DEERScan", "Cholesky", "cholesky",
 ]

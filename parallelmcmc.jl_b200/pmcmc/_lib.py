@@ -23,7 +23,7 @@ EXEC = {"fused": 0, "plain": 1}
 SYMBOLS = [
     "pmcmc_abi_version", "pmcmc_create", "pmcmc_destroy", "pmcmc_last_error",
     "pmcmc_target_diag_gauss", "pmcmc_target_dense_gauss", "pmcmc_target_logistic",
-    "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
+    "pmcmc_target_mass", "pmcmc_target_destroy", "pmcmc_tape", "pmcmc_deer_solve", "pmcmc_sample",
     "pmcmc_affine_scan_diag", "pmcmc_set_profiling", "pmcmc_get_profile",
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
     "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
@@ -114,6 +114,7 @@ def load(path: str = LIB_PATH):
             getattr(L, fn).argtypes = [_vp, C.c_int64, _vp, _vp, C.POINTER(_vp)]
         L.pmcmc_target_logistic.argtypes = [_vp, C.c_int64, C.c_int64, _vp, _vp, C.c_double,
                                             C.POINTER(_vp)]
+        L.pmcmc_target_mass.argtypes = [_vp, _vp, _vp, C.POINTER(_vp)]
         L.pmcmc_target_destroy.argtypes = [_vp]
         L.pmcmc_tape.argtypes = [_vp, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64, _vp, _vp,
                                  C.c_int32]

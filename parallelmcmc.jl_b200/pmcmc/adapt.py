@@ -34,7 +34,7 @@ import numpy as np
 
 from . import _lib as L
 from ._lib import ArgumentError
-from .core import DensityModel, ParallelMALASampler, adjoint, solve
+from .core import Cholesky, DensityModel, ParallelMALASampler, _mass_factor, adjoint, solve
 
 
 @dataclass
@@ -63,7 +63,7 @@ class AdaptiveMALASampler:
         if not (0.5 < self.kappa <= 1.0):
             raise ArgumentError(f"kappa must be in (0.5, 1], got {self.kappa}")
         if self.cholM is not None:
-            raise ArgumentError("cholM (mass matrix) is not supported by the device sampler")
+            self.cholM = Cholesky(L=_mass_factor(self.cholM))
 
 
 def dual_average_update(epsilon_init: float, epsilon_bar: float, H_bar: float, m: int,
@@ -130,6 +130,11 @@ def adapt_step_size(model: DensityModel, sampler: ParallelMALASampler, x0, *,
     hist = []
     if method == "dual_averaging":
         ad = adaptive or AdaptiveMALASampler(eps)
+        if ad.cholM is not None:
+            # the adaptive sampler's mass matrix (src/interface.jl:1040) drives the blocks
+            if sampler.cholM is not None and not np.array_equal(sampler.cholM.L, ad.cholM.L):
+                raise ArgumentError("sampler and adaptive carry different mass matrices")
+            sampler = replace(sampler, cholM=ad.cholM)
         eps_bar, H_bar, m = ad.epsilon_init, 0.0, 0
         eps = used = ad.epsilon_init
         for b in range(n_blocks):

@@ -16,6 +16,7 @@ results come back as CUDA tensors.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 from dataclasses import dataclass, field
 from typing import Any, Optional, Sequence
 
@@ -39,6 +40,57 @@ def _torch_ready(x):
 
 def _dtype_code(dt) -> int:
     return L.F32 if np.dtype(dt) == np.float32 else L.F64
+
+
+# --------------------------------------------------------------------------- mass matrix
+class Cholesky:
+    """cholesky(M): the lower factor L of a symmetric positive definite mass
+    matrix M = L L^T, as the reference's `cholM = cholesky(M)` keyword takes it
+    (src/interface.jl:84-100).  `.L` is lower, `.U` = L^T."""
+
+    def __init__(self, M=None, *, L=None):
+        if (M is None) == (L is None):
+            raise ArgumentError("give the matrix M or its lower factor L")
+        if L is None:
+            Mm = np.asarray(M, dtype=np.float64)
+            if Mm.ndim != 2 or Mm.shape[0] != Mm.shape[1]:
+                raise DimensionMismatch("M must be a square matrix")
+            try:
+                L = np.linalg.cholesky(0.5 * (Mm + Mm.T))
+            except np.linalg.LinAlgError as e:
+                raise ArgumentError(f"M is not positive definite: {e}") from None
+        self.L = _mass_factor(L)
+
+    @property
+    def U(self):
+        return self.L.T
+
+    @property
+    def M(self):
+        return self.L @ self.L.T
+
+
+def cholesky(M) -> Cholesky:
+    return Cholesky(M)
+
+
+def _mass_factor(cholM, D: Optional[int] = None):
+    """The lower factor of a cholM argument (a Cholesky, anything with `.L`, or
+    a square lower-triangular array) as float64, checked."""
+    Lm = getattr(cholM, "L", cholM)
+    try:
+        Lm = np.asarray(Lm, dtype=np.float64)
+    except (TypeError, ValueError):
+        raise ArgumentError("cholM must be a Cholesky factor (cholesky(M)) or a lower "
+                            "triangular matrix") from None
+    if Lm.ndim != 2 or Lm.shape[0] != Lm.shape[1]:
+        raise DimensionMismatch("cholM must be a square factor")
+    if D is not None and Lm.shape[0] != D:
+        raise DimensionMismatch(f"cholM is {Lm.shape[0]} x {Lm.shape[0]}, the model has dim {D}")
+    Lm = np.tril(Lm)
+    if not np.all(np.isfinite(Lm)) or not np.all(np.diag(Lm) > 0):
+        raise ArgumentError("cholM must be finite with a positive diagonal")
+    return Lm
 
 
 # --------------------------------------------------------------------------- model
@@ -68,6 +120,7 @@ class DensityModel:
             raise ArgumentError("dim is required")
         self.dim = int(dim)
         self._dev: dict[int, Any] = {}
+        self._mass: dict[tuple, Any] = {}
 
     # ---- built-in device targets
     @classmethod
@@ -108,8 +161,21 @@ class DensityModel:
                    target={"kind": "logistic", "D": X.shape[1], "X": X, "y": y,
                            "prior_prec": float(prior_prec)})
 
-    def device_target(self, handle: L.Handle):
-        """pmcmc_target* on the handle's device (created once, cached)."""
+    def device_target(self, handle: L.Handle, cholM=None):
+        """pmcmc_target* on the handle's device (created once, cached); with
+        cholM, the target of the chain with that mass matrix
+        (pmcmc_target_mass), cached per factor."""
+        if cholM is not None:
+            Lm = _mass_factor(cholM, self.dim)
+            key = (id(handle), Lm.shape[0], hashlib.sha256(Lm.tobytes()).digest())
+            if key not in self._mass:
+                base = self.device_target(handle)
+                Lf = np.asfortranarray(Lm)
+                t = C.c_void_p()
+                L.check(L.load().pmcmc_target_mass(handle.ptr, base, Lf.ctypes.data, C.byref(t)),
+                        handle.ptr, "target_mass")
+                self._mass[key] = (handle, t)
+            return self._mass[key][1]
         if self.target is None:
             raise ArgumentError(
                 "the GPU sampler needs a built-in device target (DensityModel.diag_gaussian, "
@@ -152,7 +218,7 @@ class DensityModel:
 
     def __del__(self):
         try:
-            for h, t in self._dev.values():
+            for h, t in list(self._mass.values()) + list(self._dev.values()):
                 if h.ptr:
                     L.load().pmcmc_target_destroy(t)
         except Exception:
@@ -190,7 +256,7 @@ class ParallelMALASampler:
             raise ArgumentError("jacobian must be :stoch_diag, :diag or :full")
         self.jacobian = jac
         if self.cholM is not None:
-            raise ArgumentError("cholM (mass matrix) is not supported by the device sampler")
+            self.cholM = Cholesky(L=_mass_factor(self.cholM))
         if self.exec not in L.EXEC:
             raise ArgumentError("exec must be 'fused' or 'plain'")
         if self.dtype is None:
@@ -199,6 +265,10 @@ class ParallelMALASampler:
         if self.dtype not in (np.float32, np.float64):
             raise ArgumentError("dtype must be float32 or float64")
         self.epsilon = float(self.epsilon)
+
+    def target(self, model: "DensityModel", handle: L.Handle):
+        """The device target this sampler runs on `model` (with its mass matrix)."""
+        return model.device_target(handle, self.cholM)
 
     def params(self) -> L.DeerParams:
         return L.DeerParams(self.epsilon, int(self.T), int(self.maxiter), float(self.tol_abs),
@@ -281,7 +351,7 @@ def sample(model: DensityModel, sampler: ParallelMALASampler, N: int, *, seed: i
     if N < 1:
         raise ArgumentError("the number of samples must be >= 1")
     h = handle or L.default_handle(device)
-    tgt = model.device_target(h)
+    tgt = sampler.target(model, h)
     x0 = _initial_params(model, sampler, initial_params, seed)
     keep, x0p, mem = _input_vector(x0, model.dim, sampler.dtype, None)
     dev = x0.device if mem == L.MEM_DEVICE else None
@@ -366,7 +436,7 @@ def solve(model: DensityModel, sampler: ParallelMALASampler, s0, *, seed: int = 
     return_info=true): returns S (D, T), info and, with return_logp, logp (T,)
     and the accept flags (T,)."""
     h = handle or L.default_handle(device)
-    tgt = model.device_target(h)
+    tgt = sampler.target(model, h)
     keep, x0p, mem = _input_vector(s0, model.dim, sampler.dtype, None)
     dev = s0.device if mem == L.MEM_DEVICE else None
     T = int(sampler.T)
@@ -393,7 +463,7 @@ def autotune(model: DensityModel, sampler: ParallelMALASampler, x0, *, seed: int
     {"choice": kept value (CTAs a SM, or :full chunk count; 0 if nothing to
     tune), "ms": its time a solve}."""
     h = handle or L.default_handle(device)
-    tgt = model.device_target(h)
+    tgt = sampler.target(model, h)
     keep, x0p, mem = _input_vector(x0, model.dim, sampler.dtype, None)
     ch = C.c_int32(0)
     ms = C.c_double(0.0)
@@ -412,7 +482,7 @@ def mala_chains(model: DensityModel, sampler: ParallelMALASampler, x0s, seeds, *
     tape of (seeds[c], block), the tape DEER uses for that seed and block.
     Returns S (n, T, D), logp (n, T) and accept flags (n, T)."""
     h = handle or L.default_handle(device)
-    tgt = model.device_target(h)
+    tgt = sampler.target(model, h)
     x = np.ascontiguousarray(np.asarray(x0s, dtype=sampler.dtype).reshape(-1, model.dim))
     n = x.shape[0]
     sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(-1))
@@ -444,7 +514,7 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
     if objective not in L.OBJECTIVE:
         raise ArgumentError("objective must be 'esjd' or 'mean_sq'")
     h = handle or L.default_handle(device)
-    tgt = model.device_target(h)
+    tgt = sampler.target(model, h)
     keep, x0p, mem = _input_vector(s0, model.dim, sampler.dtype, None)
     if mem == L.MEM_DEVICE:
         Sc = _torch_ready(S.T.contiguous())
@@ -490,7 +560,7 @@ def fleet_solve(chains, *, workers: int = 8, handle: Optional[L.Handle] = None, 
         keep.append(x)
         outs.append((S, lp, acc))
         c = arr[i]
-        c.target = model.device_target(h)
+        c.target = sampler.target(model, h)
         c.params = sampler.params()
         c.x0, c.seed, c.block = x.ctypes.data, int(seed), int(block)
         c.S_out, c.logp_out, c.accept_out = S.ctypes.data, lp.ctypes.data, acc.ctypes.data

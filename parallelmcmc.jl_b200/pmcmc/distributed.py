@@ -95,7 +95,7 @@ class DeviceSlice:
         self.model = model
         self.sampler = sampler
         self.h = handle
-        self.tgt = model.device_target(handle)
+        self.tgt = sampler.target(model, handle)
         self.dt = np.dtype(sampler.dtype)
         self.lib = L.load()
 

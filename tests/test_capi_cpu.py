@@ -56,6 +56,34 @@ def test_sampler_validation_mirrors_reference():
             ParallelMALASampler(**bad)
 
 
+def test_mass_matrix_arguments():
+    # cholM = cholesky(M) (interface.jl:84-100): the factor is checked up front
+    import numpy as np
+    from pmcmc import ArgumentError, Cholesky, DimensionMismatch, ParallelMALASampler, cholesky
+    from pmcmc.adapt import AdaptiveMALASampler
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((5, 5))
+    M = A @ A.T + 5 * np.eye(5)
+    c = cholesky(M)
+    assert np.allclose(c.L @ c.L.T, M) and np.allclose(c.U, c.L.T)
+    assert np.array_equal(c.L, np.tril(c.L))
+    s = ParallelMALASampler(0.1, cholM=c)
+    assert np.array_equal(s.cholM.L, c.L)
+    # a plain lower factor is accepted; the strict upper part is ignored
+    s2 = ParallelMALASampler(0.1, cholM=c.L + np.triu(np.ones((5, 5)), 1))
+    assert np.array_equal(s2.cholM.L, c.L)
+    assert np.array_equal(AdaptiveMALASampler(0.1, cholM=c).cholM.L, c.L)
+    with pytest.raises(DimensionMismatch):
+        ParallelMALASampler(0.1, cholM=np.ones((2, 3)))
+    with pytest.raises(ArgumentError):
+        ParallelMALASampler(0.1, cholM=np.diag([1.0, 0.0, 1.0]))
+    with pytest.raises(ArgumentError):
+        Cholesky(-np.eye(3))
+    with pytest.raises(DimensionMismatch):
+        from pmcmc.core import _mass_factor
+        _mass_factor(c, 4)
+
+
 def test_model_requires_device_target():
     import numpy as np
     from pmcmc import ArgumentError, DensityModel, DimensionMismatch

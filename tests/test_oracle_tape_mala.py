@@ -156,3 +156,55 @@ def test_full_jacobian_matches_jvp_and_batched():
             f2, jv = O.fwd_and_jvp(tg, eps, X[:, t], Xi[:, t], u[t], Z[:, t])
             assert np.max(np.abs(J @ Z[:, t] - jv)) < 1e-12
             assert np.max(np.abs(Jt[:, t] - jv)) < 1e-12 and np.array_equal(FT[:, t], f)
+
+
+# mass matrix of test-MALA-Kernel.jl:199-204 (D = 3, eps = 0.08, standard normal target)
+M_REF = np.array([[1.7, 0.2, -0.1], [0.2, 1.3, 0.15], [-0.1, 0.15, 1.5]])
+
+
+def test_mass_step_matches_reference_formulas():
+    # test-MALA-Kernel.jl:199-217: y = x + eps L L^T g + sqrt(2 eps) L xi, and log q with
+    # M^-1 and log det M (test-MALA-Kernel.jl:26-36)
+    rng = np.random.default_rng(20260201)
+    D, eps = 3, 0.08
+    Lf = np.linalg.cholesky(M_REF)
+    tg, _ = _std_normal(D)
+    x, xi = rng.standard_normal(D), rng.standard_normal(D)
+    S, acc, la = O.mala_sequential_mass(tg, eps, Lf, x, xi[:, None], np.array([1e-300]))
+    y = x + eps * (Lf @ (Lf.T @ -x)) + np.sqrt(2 * eps) * (Lf @ xi)
+    assert acc[0] and np.max(np.abs(S[:, 0] - y)) < 1e-12
+
+    def lq(a, b, gb):
+        r = a - b - eps * (M_REF @ gb)
+        return (-0.5 * r @ np.linalg.solve(M_REF, r) / (2 * eps) - D / 2 * np.log(4 * np.pi * eps)
+                - 0.5 * np.linalg.slogdet(M_REF)[1])
+
+    ref = (-0.5 * y @ y + lq(x, y, -y)) - (-0.5 * x @ x + lq(y, x, -x))
+    assert abs(la[0] - ref) <= 1e-10 + 1e-10 * abs(ref)
+
+
+def test_mass_chain_is_the_whitened_chain():
+    # the identity the device solve is built on: MALA with mass M = L L^T from x0 is
+    # L times plain MALA on the whitened target (precision L^T P L, mean L^-1 mu) from
+    # L^-1 x0, on the same tape, with the same log alpha
+    rng = np.random.default_rng(8)
+    D, T, eps = 6, 200, 0.25
+    A = rng.standard_normal((D, D))
+    P = A @ A.T / D + np.eye(D)
+    mu = rng.standard_normal(D)
+    B = rng.standard_normal((D, D))
+    # eps * lambda_max(L^T P L) = 0.6: a stable chain, so roundoff does not grow
+    Lf = np.linalg.cholesky(0.25 * (B @ B.T / D + 0.5 * np.eye(D)))
+    Xi, u = O.tape(5, 0, D, T)
+    x0 = rng.standard_normal(D)
+    S, acc, la = O.mala_sequential_mass(O.Target.dense_gauss(P, mu), eps, Lf, x0, Xi, u)
+    Pw = Lf.T @ P @ Lf
+    tw = O.Target.dense_gauss(0.5 * (Pw + Pw.T), np.linalg.solve(Lf, mu))
+    Sw, accw, law = O.mala_sequential(tw, eps, np.linalg.solve(Lf, x0), Xi, u)
+    assert 0 < (~acc).sum() < T and np.array_equal(acc, accw)
+    assert np.max(np.abs(S - Lf @ Sw)) < 1e-11
+    assert np.max(np.abs(la - law)) < 1e-10
+    # identity factor: the plain chain, bit for bit
+    S1, acc1, la1 = O.mala_sequential_mass(O.Target.dense_gauss(P, mu), eps, np.eye(D), x0, Xi, u)
+    S0, acc0, la0 = O.mala_sequential(O.Target.dense_gauss(P, mu), eps, x0, Xi, u)
+    assert np.array_equal(acc1, acc0) and np.max(np.abs(S1 - S0)) < 1e-14
