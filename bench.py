@@ -29,6 +29,7 @@ Secondary measurements (1 GPU):
     python bench.py --workload aniso_diag_d100       # D=100, T=16384, :diag (persistent kernel)
     python bench.py --workload corr_gauss_d64_full   # D=64, T=8192, :full
     python bench.py --workload logistic_fleet        # 32 uneven logistic chains (N, T / 4)
+    python bench.py --workload logistic_fleet_full   # all 512 chains at full N and T
     python bench.py --workload logistic_n10k_d256 --dim 512   # the wide tensor-core pass
 --small shrinks T (logistic 4096, correlated Gaussian 1024) for profiler captures.
 """
@@ -684,6 +685,8 @@ def run_fleet(args):
 
     n = 8 if args.small else 32
     chains = configs.logistic_fleet(n_chains=n, scale=0.25)
+    if dist_setup()[0] > 1:
+        return run_fleet_ranks(args, chains, f"logistic_fleet_{n}chains_scale0.25")
     h = pmcmc.Handle(0)
     total_T = sum(s.T for _, s, *_ in chains)
     # stiff chains (small D, large N: eps * lambda_max > 2) can diverge in DEER itself,
@@ -740,6 +743,168 @@ def run_fleet(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fleet_ranks(args, chains, workload):
+    """The fleet on N GPUs, one process each: every rank solves the chains the
+    cost-balanced partition gives it (pmcmc.distributed.fleet_solve_distributed,
+    no collective while they solve); the time is the slowest rank's."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import pmcmc
+    from pmcmc import distributed as Dd
+
+    world, rank, local = dist_setup()
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    h = pmcmc.Handle(local)
+    solve = lambda cs: pmcmc.fleet_solve(cs, workers=8, handle=h, errors="report")
+    Dd.fleet_solve_distributed(chains, gather=False, solve=solve)  # warm-up
+    times, mine = [], {}
+    with ClockSampler(local) as clk:
+        for _ in range(max(1, args.steps)):
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            mine = Dd.fleet_solve_distributed(chains, gather=False, solve=solve)
+            torch.cuda.synchronize(dev)
+            t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            times.append(float(t.item()))
+    ok = torch.tensor([sum(chains[i][1].T for i, r in mine.items() if r[1]["converged"]),
+                       sum(1 for r in mine.values() if r[1]["converged"]),
+                       sum(1 for r in mine.values() if r[1]["status"] == 4)],
+                      dtype=torch.float64, device=dev)
+    dist.all_reduce(ok)
+    best = min(times)
+    clocks = clk.summary()
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank != 0:
+        return
+    total_T = sum(s.T for _, s, *_ in chains)
+    line = {"metric": METRIC, "secondary": True, "value": total_T / best, "unit": "samples/s",
+            "n_gpus": world, "steps": len(times), "warmup": 1, "ms_per_step": 1e3 * best,
+            "higher_is_better": True, "scaling": "strong", "dtype": "f32",
+            "data": "synthetic (seeded NumPy PCG64 per chain + counter-based Philox tape)",
+            "timing": "host wall clock around each rank's share with device synchronisation, "
+                      "max over ranks (all_reduce), best of the timed runs",
+            "config": {"workload": workload, "chains": len(chains), "T_total": total_T,
+                       "parallelism": f"chains partitioned over {world} GPUs (longest first)",
+                       "converged": int(ok[1].item()), "nonfinite": int(ok[2].item()),
+                       "T_converged": int(ok[0].item())},
+            "clocks_rank0": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def run_fleet_full(args):
+    """All 512 chains of the uneven logistic fleet at full N and T (chain c: seed c,
+    D uniform on {16, ..., 512}, N in [1000, 20000], T in [1024, 32768], :stoch_diag,
+    eps adapted per chain from 0.5 / sqrt(D) by dual averaging over short blocks),
+    solved through pmcmc_fleet_solve on 8 worker streams in batches of 64 chains
+    (the data of all 512 would take ~11 GB of host memory); the plain per-chain
+    FP32 path on 16 chains against the same chains on the fleet."""
+    import numpy as np
+    import torch
+
+    import pmcmc
+    from pmcmc import configs
+
+    from pmcmc.adapt import adapt_fleet
+
+    n_total, batch = (64, 32) if args.small else (512, 64)
+    rounds, t_adapt = 12, 128
+    h = pmcmc.Handle(0)
+    pmcmc.fleet_solve(configs.logistic_fleet(n_chains=4, scale=0.05), workers=4, handle=h,
+                      errors="report")  # warm-up
+    per, total_s, adapt_s = [], 0.0, 0.0
+    sub = None
+    with ClockSampler(0) as clk:
+        for b0 in range(0, n_total, batch):
+            chains0 = configs.logistic_fleet(n_chains=min(batch, n_total - b0), first=b0)
+            for m, *_ in chains0:  # device targets outside the timed region
+                m.device_target(h)
+            # per-chain step size: dual averaging from eps = 0.5 / sqrt(D) over short
+            # blocks of the whole batch, the chain moving on from block to block
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            chains, hist = adapt_fleet(chains0, rounds=rounds, T_adapt=t_adapt, handle=h)
+            torch.cuda.synchronize()
+            adapt_s += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            res = pmcmc.fleet_solve(chains, workers=8, handle=h, errors="report")
+            torch.cuda.synchronize()
+            total_s += time.perf_counter() - t0
+            for (m, smp, *_), (_, s0, *_), r, hc in zip(chains, chains0, res, hist):
+                per.append({"D": m.dim, "N": m.target["X"].shape[0], "T": smp.T,
+                            "eps0": s0.epsilon, "eps": smp.epsilon,
+                            "adapt_rates": [round(a, 3) for _, a in hc[-3:]],
+                            "iters": r[1]["iters"], "converged": bool(r[1]["converged"]),
+                            "status": r[1]["status"],
+                            "accept": float(np.mean(r[3])) if r[3] is not None else None})
+            if b0 == 0:
+                sub = chains[:16]
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                rf = pmcmc.fleet_solve(sub, workers=8, handle=h, errors="report")
+                torch.cuda.synchronize()
+                sub_fleet = time.perf_counter() - t0
+                plain = [(m, dataclasses.replace(smp, exec="plain"), *rest)
+                         for m, smp, *rest in sub]
+                t0 = time.perf_counter()
+                rp = pmcmc.fleet_solve(plain, workers=1, handle=h, errors="report")
+                torch.cuda.synchronize()
+                sub_plain = time.perf_counter() - t0
+                sub_T = sum(smp.T for _, smp, *_ in sub)
+                sub_ok = [bool(a[1]["converged"]) and bool(b[1]["converged"])
+                          for a, b in zip(rf, rp)]
+                sub_stats = {"chains": len(sub), "T_total": sub_T,
+                             "fleet": {"value": sub_T / sub_fleet, "unit": "samples/s",
+                                       "converged": sum(bool(r[1]["converged"]) for r in rf)},
+                             "plain_per_chain": {"value": sub_T / sub_plain, "unit": "samples/s",
+                                                 "converged": sum(bool(r[1]["converged"])
+                                                                  for r in rp)},
+                             "speedup_fleet_over_plain": sub_plain / sub_fleet,
+                             "both_converged": sum(sub_ok)}
+                del rf, rp, plain
+            del chains, res
+    ok = [c for c in per if c["converged"] and c["status"] == 0]
+    samples = sum(c["T"] for c in ok)
+    line = {"metric": METRIC, "secondary": True, "value": samples / total_s, "unit": "samples/s",
+            "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * total_s,
+            "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded NumPy PCG64 per chain + counter-based Philox tape)",
+            "timing": "host wall clock around each batch's pmcmc_fleet_solve with device "
+                      "synchronisation (host outputs), summed over the batches; only "
+                      "converged chains count as samples; the step-size adaptation before "
+                      "it is timed apart (adaptation_s, value_with_adaptation)",
+            "adaptation_s": adapt_s,
+            "value_with_adaptation": samples / (total_s + adapt_s),
+            "config": {"workload": f"logistic_fleet_{n_total}chains_full", "chains": n_total,
+                       "batch": batch, "workers": 8,
+                       "adaptation": f"dual averaging, {rounds} rounds of {t_adapt}-step blocks "
+                                     f"per chain from eps = 0.5 / sqrt(D)",
+                       "T_total_all": sum(c["T"] for c in per), "T_total_converged": samples,
+                       "converged": len(ok),
+                       "not_converged": sum(1 for c in per if not c["converged"] and
+                                            c["status"] == 0),
+                       "nonfinite": [i for i, c in enumerate(per) if c["status"] == 4],
+                       "newton_iters": {"min": min(c["iters"] for c in per),
+                                        "median": statistics.median(c["iters"] for c in per),
+                                        "max": max(c["iters"] for c in per)},
+                       "accept_rate_median": statistics.median(
+                           c["accept"] for c in per if c["accept"] is not None),
+                       "eps_over_eps0_median": statistics.median(c["eps"] / c["eps0"]
+                                                                 for c in per)},
+            "subset_vs_plain": sub_stats,
+            "per_chain": per,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -753,7 +918,7 @@ def main():
                     help="skip the secondary diagonal-Gaussian measurements")
     ap.add_argument("--workload", default="logistic_n10k_d256",
                     choices=["logistic_n10k_d256", "aniso_diag_d100", "corr_gauss_d64_full",
-                             "logistic_fleet"])
+                             "logistic_fleet", "logistic_fleet_full"])
     ap.add_argument("--dim", type=int, default=256,
                     help="logistic workload: dimension D (256 < D <= 512 runs the wide "
                          "tensor-core pass); D != 256 or --small is a secondary line")
@@ -766,6 +931,8 @@ def main():
         run_reference(args)
     elif args.workload == "logistic_fleet":
         run_fleet(args)
+    elif args.workload == "logistic_fleet_full":
+        run_fleet_full(args)
     elif args.workload == "aniso_diag_d100":
         run_gauss(args)
     elif args.workload == "corr_gauss_d64_full" or args.small or args.dim != 256:

@@ -327,6 +327,30 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_p
                       int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
                       void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem);
 
+/* pmcmc_mala_chains_adaptive: the same chains as AdaptiveMALASampler runs them
+ * (src/interface.jl:899-933 settings, 1024-1065 step): chain c carries its own
+ * step size, epsilon_init = p->epsilon.  Step m (0-based) uses epsilon while
+ * m < n_warmup and epsilon_bar after, and during warmup is followed by the
+ * dual-averaging update _dual_average_update (src/interface.jl:962-984) with
+ * that step's log alpha and m + 1.  The settings are checked as the
+ * reference's constructor checks them (PMCMC_ERR_ARGUMENT).  Extra outputs
+ * (either may be NULL; host or device per mem): eps_out n x T, the step size
+ * of every step (the transition's step_size; is_warmup = m < n_warmup), and
+ * state_out n x 3, the final (epsilon, epsilon_bar, H_bar) of every chain.
+ * The adaptation is computed in FP64 whatever p->dtype. */
+typedef struct pmcmc_adapt {
+  int64_t n_warmup;     /* 1000 in the reference */
+  double target_accept; /* 0.574 */
+  double gamma;         /* 0.05 */
+  double t0;            /* 10.0 */
+  double kappa;         /* 0.75 */
+} pmcmc_adapt;
+int pmcmc_mala_chains_adaptive(pmcmc_handle* h, const pmcmc_target* t,
+                               const pmcmc_deer_params* p, int64_t n, const void* x0,
+                               const uint64_t* seeds, uint64_t block, const pmcmc_adapt* ad,
+                               void* S_out, void* logp_out, uint8_t* accept_out,
+                               double* eps_out, double* state_out, int32_t mem);
+
 /* pmcmc_autotune (no counterpart in the reference): times the candidate
  * shapes of the kernels that would solve (t, p) on x0 and keeps the fastest
  * for every later solve of the same shape (target kind, Jacobian, precision, D,

@@ -15,6 +15,7 @@ bayes_logreg.jl.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -224,6 +225,44 @@ def mala_sequential(tg, eps, x0, Xi, u):
     lib().orc_mala_sequential(tg.ref(), eps, _p(x0), _p(Xi_c), _p(u), T, _p(S),
                               _p(acc, _ip), _p(la))
     return S.T, acc.astype(bool), la
+
+
+def dual_average(eps_init, eps_bar, h_bar, m, la, target_accept=0.574, gamma=0.05, t0=10.0,
+                 kappa=0.75):
+    """_dual_average_update (src/interface.jl:962-984): (eps, eps_bar, H_bar)
+    after step m (m >= 1) with log acceptance ratio la."""
+    alpha = 1.0 if la >= 0 else math.exp(la)
+    mu = math.log(10.0 * eps_init)
+    w = 1.0 / (m + t0)
+    h_new = (1.0 - w) * h_bar + w * (target_accept - alpha)
+    log_eps = mu - math.sqrt(m) / gamma * h_new
+    mk = m ** (-kappa)
+    log_eps_bar = mk * log_eps + (1.0 - mk) * math.log(eps_bar)
+    return math.exp(log_eps), math.exp(log_eps_bar), h_new
+
+
+def mala_adaptive(tg, eps_init, x0, Xi, u, n_warmup, **settings):
+    """AdaptiveMALASampler's chain (src/interface.jl:1024-1065) on a fixed tape:
+    step m uses eps while m < n_warmup and eps_bar after, and during warmup is
+    followed by dual_average with m + 1.  Returns S (D, T), accepted (T,),
+    step sizes (T,) and the final (eps, eps_bar, H_bar)."""
+    Xi_c = _col(Xi)
+    T, D = Xi_c.shape
+    x = np.asarray(x0, np.float64)
+    eps = eps_bar = float(eps_init)
+    h_bar = 0.0
+    S = np.empty((D, T))
+    acc = np.empty(T, bool)
+    used = np.empty(T)
+    for t in range(T):
+        warm = t < n_warmup
+        e = eps if warm else eps_bar
+        x, acc[t], la = mala_step(tg, e, x, Xi_c[t], float(u[t]))
+        if warm:
+            eps, eps_bar, h_bar = dual_average(eps_init, eps_bar, h_bar, t + 1, la, **settings)
+        S[:, t] = x
+        used[t] = e
+    return S, acc, used, (eps, eps_bar, h_bar)
 
 
 def mala_sequential_mass(tg, eps, Lfac, x0, Xi, u):

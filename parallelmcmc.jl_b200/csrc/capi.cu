@@ -2209,9 +2209,16 @@ int pmcmc_affine_scan_diag(pmcmc_handle* h, int32_t dtype, int64_t D, int64_t T,
   return PMCMC_OK;
 }
 
-int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
-                      int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
-                      void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem) {
+}  // extern "C"
+
+namespace {
+
+// Sequential chains, fixed or adaptive step size (ad == nullptr: fixed).
+int chains_impl(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p, int64_t n,
+                const void* x0, const uint64_t* seeds, uint64_t block, const pmcmc_adapt* ad,
+                void* S_out, void* logp_out, uint8_t* accept_out, double* eps_out,
+                double* state_out, int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
   int rc = validate(h, tg, p);
   if (rc) return rc;
   if (!x0 || !seeds || !S_out)
@@ -2243,19 +2250,34 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
   P.prec_d = tg->prec_d;
   P.mean_f = tg->mean_f;
   P.prec_f = tg->prec_f;
+  ChainAdapt cad{};
+  if (ad) {
+    // AdaptiveMALASampler's checks (src/interface.jl:919-923)
+    if (!(ad->target_accept > 0 && ad->target_accept < 1))
+      return fail(h, PMCMC_ERR_ARGUMENT, "target_accept must be in (0,1), got %g",
+                  ad->target_accept);
+    if (!(ad->gamma > 0)) return fail(h, PMCMC_ERR_ARGUMENT, "gamma must be > 0, got %g", ad->gamma);
+    if (!(ad->t0 > 0)) return fail(h, PMCMC_ERR_ARGUMENT, "t0 must be > 0, got %g", ad->t0);
+    if (!(ad->kappa > 0.5 && ad->kappa <= 1.0))
+      return fail(h, PMCMC_ERR_ARGUMENT, "kappa must be in (0.5, 1], got %g", ad->kappa);
+    if (ad->n_warmup < 0) return fail(h, PMCMC_ERR_ARGUMENT, "n_warmup must be >= 0");
+    cad = ChainAdapt{1, ad->n_warmup, ad->target_accept, ad->gamma, ad->t0, ad->kappa};
+  }
   const void* dx0 = x0;
   const uint64_t* dseeds = seeds;
   void *dS = S_out, *dlp = logp_out;
   uint8_t* dacc = accept_out;
+  double *deps = eps_out, *dst = state_out;
   const size_t bx = es * n * D, bs = 8 * static_cast<size_t>(n), bS = es * n * T * D,
-               blp = logp_out ? es * n * T : 0, bacc = accept_out ? n * T : 0;
+               blp = logp_out ? es * n * T : 0, bacc = accept_out ? n * T : 0,
+               beps = eps_out ? 8 * n * T : 0, bst = state_out ? 24 * static_cast<size_t>(n) : 0;
   // mass-matrix targets: the chains run whitened from x0' = L^-1 x0 (the
   // solve's whitening, solve_mass), and map back in place after the launch
   const bool mass = tg->mass_Ld != nullptr;
   auto a = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t bw = mass ? a(bx) : 0;
   if (mem == PMCMC_MEM_HOST) {
-    rc = ensure_ws(h, bw + a(bx) + a(bs) + a(bS) + a(blp) + a(bacc));
+    rc = ensure_ws(h, bw + a(bx) + a(bs) + a(bS) + a(blp) + a(bacc) + a(beps) + a(bst));
     if (rc) return rc;
     unsigned char* w = h->ws + bw;
     dx0 = w;
@@ -2263,6 +2285,9 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
     dS = w + a(bx) + a(bs);
     dlp = logp_out ? w + a(bx) + a(bs) + a(bS) : nullptr;
     dacc = accept_out ? w + a(bx) + a(bs) + a(bS) + a(blp) : nullptr;
+    unsigned char* w2 = w + a(bx) + a(bs) + a(bS) + a(blp) + a(bacc);
+    deps = eps_out ? reinterpret_cast<double*>(w2) : nullptr;
+    dst = state_out ? reinterpret_cast<double*>(w2 + a(beps)) : nullptr;
     CK(cudaMemcpyAsync(const_cast<void*>(dx0), x0, bx, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(const_cast<uint64_t*>(dseeds), seeds, bs, cudaMemcpyHostToDevice,
                        h->stream));
@@ -2274,16 +2299,41 @@ int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_
     CK(mass_whiten(h->stream, tg->mass_Ld, D, n, dx0, h->ws, f64));
     dx0 = h->ws;
   }
-  CK(launch_mala_chains(h->stream, f64, tg->kind, P, n, dx0, dseeds, dS, dlp, dacc));
+  CK(launch_mala_chains(h->stream, f64, tg->kind, P, cad, n, dx0, dseeds, dS, dlp, dacc, deps,
+                        dst));
   if (mass) CK(mass_map(h->stream, tg->mass_Ld, D, n * T, dS, f64, h->num_sms));
   if (mem == PMCMC_MEM_HOST) {
     CK(cudaMemcpyAsync(S_out, dS, bS, cudaMemcpyDeviceToHost, h->stream));
     if (logp_out) CK(cudaMemcpyAsync(logp_out, dlp, blp, cudaMemcpyDeviceToHost, h->stream));
     if (accept_out)
       CK(cudaMemcpyAsync(accept_out, dacc, bacc, cudaMemcpyDeviceToHost, h->stream));
+    if (eps_out) CK(cudaMemcpyAsync(eps_out, deps, beps, cudaMemcpyDeviceToHost, h->stream));
+    if (state_out) CK(cudaMemcpyAsync(state_out, dst, bst, cudaMemcpyDeviceToHost, h->stream));
   }
   CK(cudaStreamSynchronize(h->stream));
   return PMCMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmcmc_mala_chains(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                      int64_t n, const void* x0, const uint64_t* seeds, uint64_t block,
+                      void* S_out, void* logp_out, uint8_t* accept_out, int32_t mem) {
+  return chains_impl(h, tg, p, n, x0, seeds, block, nullptr, S_out, logp_out, accept_out, nullptr,
+                     nullptr, mem);
+}
+
+int pmcmc_mala_chains_adaptive(pmcmc_handle* h, const pmcmc_target* tg,
+                               const pmcmc_deer_params* p, int64_t n, const void* x0,
+                               const uint64_t* seeds, uint64_t block, const pmcmc_adapt* ad,
+                               void* S_out, void* logp_out, uint8_t* accept_out,
+                               double* eps_out, double* state_out, int32_t mem) {
+  if (!h) return PMCMC_ERR_ARGUMENT;
+  if (!ad) return fail(h, PMCMC_ERR_ARGUMENT, "adaptation settings must not be NULL");
+  return chains_impl(h, tg, p, n, x0, seeds, block, ad, S_out, logp_out, accept_out, eps_out,
+                     state_out, mem);
 }
 
 int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q) {

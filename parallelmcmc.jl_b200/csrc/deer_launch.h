@@ -43,11 +43,21 @@ SmemPlan gauss_sweep_smem(bool f64, int64_t Dp, int TT, bool dense);
 
 // Independent sequential MALA chains, one warp a chain (mala_chains.cu): chain c
 // from x0[c * D ..] with the tape of (seeds[c], P.block); S is nchains x T x D.
+// With ad.active every chain adapts its step size by dual averaging from
+// epsilon_init = P.eps; eps_out (nchains x T, or nullptr) gets the step size of
+// every step and state_out (nchains x 3, or nullptr) the final (epsilon,
+// epsilon_bar, H_bar).
 struct DevParams;
+struct ChainAdapt {
+  int active;
+  int64_t n_warmup;
+  double target_accept, gamma, t0, kappa;
+};
 size_t mala_chains_smem(bool f64, int64_t Dp, bool dense);
 cudaError_t launch_mala_chains(cudaStream_t s, bool f64, int tk, const DevParams& P,
-                               int64_t nchains, const void* x0, const uint64_t* seeds, void* S,
-                               void* logp, uint8_t* acc);
+                               const ChainAdapt& ad, int64_t nchains, const void* x0,
+                               const uint64_t* seeds, void* S, void* logp, uint8_t* acc,
+                               double* eps_out, double* state_out);
 
 // Tape materialisation (tape.cu).
 cudaError_t launch_tape(cudaStream_t s, int64_t D, int64_t T, uint64_t seed, uint64_t block,

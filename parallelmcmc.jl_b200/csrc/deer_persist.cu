@@ -12,10 +12,13 @@
 //    maps S_{t0} to S_{t0 + ncols}, the first column of the next CTA.
 //  - Column 0 depends on x0 alone: S_0 = f(x0) in every sweep; CTA 0 forms it
 //    once and it seeds the scan over the group aggregates.
-//  - Per sweep: evaluate + tile scan, grid barrier, per-coordinate scan of the
-//    group aggregates (state entering every CTA), grid barrier, apply with
-//    damping in shared memory, max|dS| / max|S| atomics, grid barrier, and the
-//    convergence test (DEER.jl:567-578) read by every CTA alike.
+//  - Per sweep: evaluate + tile scan, grid barrier, the previous sweep's
+//    convergence test (DEER.jl:567-578) read by every CTA alike, per-coordinate
+//    scan of the group aggregates (state entering every CTA), grid barrier,
+//    apply with damping in shared memory, max|dS| / max|S| atomics.  Testing a
+//    sweep after the next sweep's first barrier saves a barrier a sweep; the
+//    evaluation after the last sweep is discarded.  Sweep 0 is tested at once
+//    after a third barrier, so a one-sweep solve evaluates once.
 //  - After the last sweep every CTA verifies its columns (exact MALA step from
 //    S_{t-1}, FP64 log-acceptance), writes S, logp(S_t) and the accept flags
 //    (_trajectory_logps, interface.jl:517-524), as the finalize kernel does.
@@ -200,11 +203,32 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
     int iter = 0, converged = 0, status = 0;
     Real sprev = 0;
     double metric = 0.0;
+    // the test of sweep k from its maxima (slot k & 1), after a grid barrier that
+    // follows sweep k's apply; on a stop, S_{t0 - 1} (the previous CTA's last
+    // column) is read for the verification
+    auto stop_test = [&](int k) {
+      const unsigned long long* sl = red + 3 * (k & 1);
+      const double dmax = __longlong_as_double(static_cast<long long>(__ldcg(sl)));
+      const double smax = __longlong_as_double(static_cast<long long>(__ldcg(sl + 1)));
+      const bool nonfinite = __ldcg(sl + 2) != 0ull;
+      metric = dmax / (P.tol_abs + P.tol_rel * smax);
+      converged = metric <= 1.0;
+      status = nonfinite ? static_cast<int>(kStNonfinite) : 0;
+      const bool stop = converged || iter >= P.maxiter || status != 0;
+      if (stop && cta > 0 && tid < Dp) sprev = __ldcg(Sb + (t0 - 1) * Dp + tid);
+      return stop;
+    };
     for (;;) {
       // ---- evaluate the scan group: column t0 + c + 1 from S_{t0 + c} ----
       // (warp-uniform loop over groups of CPW columns; a slot past the end
-      // repeats the group's first column and stores nothing)
-      for (int cb = warp * CPW; cb < ng; cb += kWarps * CPW) {
+      // repeats the group's first column and stores nothing).  The previous
+      // sweep's convergence test comes after the next grid barrier, so this
+      // evaluation runs before it is known whether another sweep is needed: a
+      // solve of more than one sweep evaluates once more than it sweeps, and a
+      // sweep has two grid barriers instead of three.  At maxiter nothing is
+      // evaluated.
+      const bool sweep = iter < P.maxiter;
+      for (int cb = warp * CPW; sweep && cb < ng; cb += kWarps * CPW) {
         const bool valid = cb + half < ng;
         const int c = valid ? cb + half : cb;
         const int t = static_cast<int>(t0 + c + 1);
@@ -233,17 +257,26 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
           }
         }
       }
-      __syncthreads();
-      tile_scan_inplace<Real>(sm.As, sm.Bs, ng, D, Dp);
-      __syncthreads();
-      for (int d = tid; d < D; d += kThreads) {
-        agg_a[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.As[(ng - 1) * Dp + d] : Real(1);
-        agg_b[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.Bs[(ng - 1) * Dp + d] : Real(0);
+      if (sweep) {
+        __syncthreads();
+        tile_scan_inplace<Real>(sm.As, sm.Bs, ng, D, Dp);
+        __syncthreads();
+        for (int d = tid; d < D; d += kThreads) {
+          agg_a[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.As[(ng - 1) * Dp + d] : Real(1);
+          agg_b[static_cast<size_t>(cta) * Dp + d] = ng > 0 ? sm.Bs[(ng - 1) * Dp + d] : Real(0);
+        }
       }
       grid.sync();
-      // every CTA has read the previous sweep's slot: clear it for the next sweep
+
+      // ---- convergence test of the previous sweep (DEER.jl:567-578), the same in
+      // every CTA: its maxima are complete, every CTA having applied it.  Sweep 0
+      // was tested at once, after a barrier of its own (below) ----
+      if (iter >= 2 && stop_test(iter - 1)) break;
+      // this sweep's slot was last read in the test of sweep iter - 2, which
+      // every CTA finished before the previous sweep's second barrier: clear it
+      // (the next barrier orders the clear before this sweep's atomics)
       if (cta == 0 && tid == 0)
-        for (int i = 0; i < 3; ++i) red[3 * ((iter + 1) & 1) + i] = 0ull;
+        for (int i = 0; i < 3; ++i) red[3 * (iter & 1) + i] = 0ull;
 
       // ---- state entering every CTA: scan of the group aggregates per coordinate ----
       for (int d = cta; d < D; d += nctas)
@@ -310,20 +343,13 @@ __global__ void __launch_bounds__(kThreads, kPersistMinBlocks<Real, QPL>)
         atomicMax(slot + 1, dbits(b));
         if (c != 0.0) atomicMax(slot + 2, 1ull);
       }
-      grid.sync();
-      // S_{t0 - 1} (the previous CTA's last column) for the verification, should
-      // this sweep be the last: its load overlaps the test's
-      if (cta > 0 && tid < Dp) sprev = __ldcg(Sb + (t0 - 1) * Dp + tid);
-
-      // ---- convergence test (DEER.jl:567-578), the same in every CTA ----
-      const double dmax = __longlong_as_double(static_cast<long long>(__ldcg(slot)));
-      const double smax = __longlong_as_double(static_cast<long long>(__ldcg(slot + 1)));
-      const bool nonfinite = __ldcg(slot + 2) != 0ull;
-      metric = dmax / (P.tol_abs + P.tol_rel * smax);
       ++iter;
-      converged = metric <= 1.0;
-      status = nonfinite ? static_cast<int>(kStNonfinite) : 0;
-      if (converged || iter >= P.maxiter || status != 0) break;
+      // the first sweep is tested at once: a block that converges in one sweep
+      // (no accepted move) then evaluates nothing more
+      if (iter == 1) {
+        grid.sync();
+        if (stop_test(0)) break;
+      }
     }
 
     // ---- verification pass and outputs on the CTA's columns ----

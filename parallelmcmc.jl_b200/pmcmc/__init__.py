@@ -7,7 +7,8 @@ from types import SimpleNamespace
 
 from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupported,
                    default_handle, load)
-from .adapt import AdaptiveMALASampler, adapt_step_size, dual_average_update
+from .adapt import (AdaptiveMALASampler, adapt_step_size, adaptive_chains, dual_average_update,
+                    sample_adaptive)
 from .core import (Chain, Cholesky, DensityModel, ParallelMALASampler, ParallelMALAState,
                    ParallelMALATransition, adjoint, autotune, fleet_solve, mala_chains, sample,
                    solve,
@@ -22,5 +23,6 @@ __all__ = [
     "default_handle", "load", "Chain", "DensityModel", "ParallelMALASampler",
     "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
     "step", "tape", "mala_chains", "autotune", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
+    "adaptive_chains", "sample_adaptive",
     "solve_affine_scan_diag", "DEER", "DEERScan", "Cholesky", "cholesky",
 ]

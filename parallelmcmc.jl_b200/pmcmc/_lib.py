@@ -28,6 +28,7 @@ SYMBOLS = [
     "pmcmc_affine_scan_diag_noalloc", "pmcmc_target_eigen", "pmcmc_deer_adjoint",
     "pmcmc_slice_begin", "pmcmc_slice_local", "pmcmc_slice_finish", "pmcmc_slice_result",
     "pmcmc_fleet_solve", "pmcmc_check_wait_bound", "pmcmc_mala_chains", "pmcmc_autotune",
+    "pmcmc_mala_chains_adaptive",
 ]
 OBJECTIVE = {"esjd": 0, "mean_sq": 1}
 WAIT_KIND = {"lookback": 0, "mbarrier": 1}
@@ -77,6 +78,11 @@ class Info(C.Structure):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["path_names"] = [n for b, n in PATH_BITS if self.path & b]
         return d
+
+
+class Adapt(C.Structure):
+    _fields_ = [("n_warmup", C.c_int64), ("target_accept", C.c_double), ("gamma", C.c_double),
+                ("t0", C.c_double), ("kappa", C.c_double)]
 
 
 class FleetChain(C.Structure):
@@ -143,6 +149,9 @@ def load(path: str = LIB_PATH):
                                      C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         L.pmcmc_mala_chains.argtypes = [_vp, _vp, C.POINTER(DeerParams), C.c_int64, _vp, _vp,
                                         C.c_uint64, _vp, _vp, _vp, C.c_int32]
+        L.pmcmc_mala_chains_adaptive.argtypes = [_vp, _vp, C.POINTER(DeerParams), C.c_int64, _vp,
+                                                 _vp, C.c_uint64, C.POINTER(Adapt), _vp, _vp, _vp,
+                                                 _vp, _vp, C.c_int32]
         for fn in SYMBOLS:
             if fn not in ("pmcmc_last_error", "pmcmc_abi_version"):
                 getattr(L, fn).restype = C.c_int

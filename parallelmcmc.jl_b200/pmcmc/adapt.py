@@ -33,7 +33,7 @@ from typing import Any, Optional
 import numpy as np
 
 from . import _lib as L
-from ._lib import ArgumentError
+from ._lib import ArgumentError, DimensionMismatch
 from .core import Cholesky, DensityModel, ParallelMALASampler, _mass_factor, adjoint, solve
 
 
@@ -64,6 +64,86 @@ class AdaptiveMALASampler:
             raise ArgumentError(f"kappa must be in (0.5, 1], got {self.kappa}")
         if self.cholM is not None:
             self.cholM = Cholesky(L=_mass_factor(self.cholM))
+
+
+def _sampler_dtype(adaptive: "AdaptiveMALASampler"):
+    # FP = typeof(float(epsilon_init)) (src/interface.jl:925-926)
+    return np.float32 if isinstance(adaptive.epsilon_init, np.float32) else np.float64
+
+
+def adaptive_chains(model: DensityModel, adaptive: "AdaptiveMALASampler", x0s, seeds, T: int, *,
+                    block: int = 0, handle: Optional[L.Handle] = None, device: int = 0,
+                    dtype=None) -> dict:
+    """n AdaptiveMALASampler chains of T steps on the device, one warp a chain
+    (pmcmc_mala_chains_adaptive): chain c starts at x0s[c] with the tape of
+    (seeds[c], block) and adapts its own step size by dual averaging during its
+    first n_warmup steps (src/interface.jl:1024-1065).  Returns a dict with S
+    (n, T, D), logp (n, T), accepted (n, T), step_size (n, T), is_warmup (n, T)
+    and epsilon, epsilon_bar, H_bar (n,): the chains' final adaptation state."""
+    import ctypes as C
+
+    h = handle or L.default_handle(device)
+    dt = np.dtype(dtype or _sampler_dtype(adaptive)).type
+    smp = ParallelMALASampler(float(adaptive.epsilon_init), T=int(T), dtype=dt,
+                              cholM=adaptive.cholM)
+    tgt = smp.target(model, h)
+    x = np.ascontiguousarray(np.asarray(x0s, dtype=dt).reshape(-1, model.dim))
+    n = x.shape[0]
+    sd = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).reshape(-1))
+    if sd.size != n:
+        raise DimensionMismatch("one seed per chain")
+    S = np.empty((n, T, model.dim), dt)
+    lp = np.empty((n, T), dt)
+    acc = np.empty((n, T), np.uint8)
+    eps = np.empty((n, T), np.float64)
+    st = np.empty((n, 3), np.float64)
+    ad = L.Adapt(int(adaptive.n_warmup), float(adaptive.target_accept), float(adaptive.gamma),
+                 float(adaptive.t0), float(adaptive.kappa))
+    p = smp.params()
+    rc = L.load().pmcmc_mala_chains_adaptive(
+        h.ptr, tgt, C.byref(p), n, x.ctypes.data, sd.ctypes.data, int(block), C.byref(ad),
+        S.ctypes.data, lp.ctypes.data, acc.ctypes.data, eps.ctypes.data, st.ctypes.data,
+        L.MEM_HOST)
+    L.check(rc, h.ptr, "mala_chains_adaptive")
+    return {"S": S, "logp": lp, "accepted": acc.astype(bool), "step_size": eps,
+            "is_warmup": np.broadcast_to(np.arange(T) < adaptive.n_warmup, (n, T)).copy(),
+            "epsilon": st[:, 0].copy(), "epsilon_bar": st[:, 1].copy(), "H_bar": st[:, 2].copy()}
+
+
+def sample_adaptive(model: DensityModel, adaptive: "AdaptiveMALASampler", N: int, *,
+                    seed: int = 0, initial_params=None, handle: Optional[L.Handle] = None,
+                    device: int = 0, **_):
+    """sample(rng, model, AdaptiveMALASampler(...), N) (src/interface.jl:987-1065)
+    on the device: as AbstractMCMC runs it, transition 1 is the initial state
+    (log density from the model, accepted, step size epsilon_init, warmup) and
+    transitions 2..N are N - 1 adaptive MALA steps on tape block 0 of `seed`.
+    The Chain's info carries step_size, is_warmup and the final epsilon_bar."""
+    from .core import Chain, _initial_params
+
+    if N < 1:
+        raise ArgumentError("the number of samples must be >= 1")
+    dt = _sampler_dtype(adaptive)
+    x0 = np.asarray(_initial_params(model, ParallelMALASampler(1.0, dtype=dt), initial_params,
+                                    seed), dt).ravel()
+    if x0.size != model.dim:
+        raise L.DimensionMismatch(f"initial state must have length {model.dim}")
+    lp0 = model.logdensity(x0) if model.logdensity is not None else np.nan
+    vals = np.empty((N, model.dim), dt)
+    logp = np.empty(N, dt)
+    acc = np.ones(N, bool)
+    step = np.full(N, float(adaptive.epsilon_init))
+    warm = np.ones(N, bool)
+    vals[0], logp[0] = x0, lp0
+    info = {"epsilon_bar": float(adaptive.epsilon_init)}
+    if N > 1:
+        r = adaptive_chains(model, adaptive, x0[None, :], [seed], N - 1, handle=handle,
+                            device=device, dtype=dt)
+        vals[1:], logp[1:], acc[1:] = r["S"][0], r["logp"][0], r["accepted"][0]
+        step[1:], warm[1:] = r["step_size"][0], r["is_warmup"][0]
+        info = {"epsilon": float(r["epsilon"][0]), "epsilon_bar": float(r["epsilon_bar"][0]),
+                "H_bar": float(r["H_bar"][0])}
+    info.update({"step_size": step, "is_warmup": warm})
+    return Chain(vals, logp, acc, info, model.param_names)
 
 
 def dual_average_update(epsilon_init: float, epsilon_bar: float, H_bar: float, m: int,
@@ -161,3 +241,72 @@ def adapt_step_size(model: DensityModel, sampler: ParallelMALASampler, x0, *,
             log_eps += step0 / math.sqrt(b + 1.0) * math.copysign(1.0, d)
         x = np.asarray(S[:, -1], sampler.dtype).copy()
     return {"epsilon": math.exp(log_eps), "history": hist}
+
+
+def adapt_fleet(chains, *, rounds: int = 8, T_adapt: int = 256, target_accept: float = 0.574,
+                max_step_ratio: float = 4.0, retries: int = 6, workers: int = 8,
+                handle: Optional[L.Handle] = None, device: int = 0, solve=None):
+    """Per-chain dual averaging of epsilon for a fleet (`chains` as for
+    pmcmc.fleet_solve), every round one short block of every chain solved
+    together on the fleet.
+
+    Round r: chain c solves tape block `block_c + 1 + r` of its seed, T_adapt
+    steps at its current epsilon from its current state; the block's accept
+    rate feeds dual_average_update (one update a block, m = r + 1, as
+    adapt_step_size does for one chain) with epsilon_init = the chain's
+    epsilon; the chain continues from the block's last column.  The epsilon a
+    block uses stays within max_step_ratio of the chain's previous one; a block
+    that goes non-finite is solved again at half its epsilon (at most `retries`
+    times; a chain that still fails keeps its halved epsilon).  `solve`
+    replaces fleet_solve (tests).
+
+    Returns (adapted, history): the chains with sampler.epsilon = epsilon_bar
+    and x0 = the state after the last round, and per chain the list of
+    (epsilon, accept rate) of its rounds."""
+    from .core import fleet_solve
+
+    if rounds < 1 or T_adapt < 1:
+        raise ArgumentError("rounds and T_adapt must be >= 1")
+    if solve is None:
+        h = handle or L.default_handle(device)
+        solve = lambda cs: fleet_solve(cs, workers=workers, handle=h, errors="report")
+    n = len(chains)
+    eps0 = [float(s.epsilon) for _, s, *_ in chains]
+    ads = [AdaptiveMALASampler(e, target_accept=target_accept) for e in eps0]
+    eps, used, eps_bar, h_bar = list(eps0), list(eps0), list(eps0), [0.0] * n
+    x = [np.asarray(x0, s.dtype).copy() for _, s, x0, *_ in chains]
+    hist = [[] for _ in range(n)]
+    for r in range(rounds):
+        todo = list(range(n))
+        for c in todo:
+            used[c] = min(max(eps[c], used[c] / max_step_ratio), used[c] * max_step_ratio)
+        res = {}
+        for _ in range(retries + 1):
+            if not todo:
+                break
+            batch = [(chains[c][0], replace(chains[c][1], epsilon=used[c], T=int(T_adapt)), x[c],
+                      chains[c][3], chains[c][4] + 1 + r) for c in todo]
+            out = solve(batch)
+            again = []
+            for c, o in zip(todo, out):
+                if o[1].get("status", 0) == L.ERR_NONFINITE:
+                    used[c] *= 0.5
+                    again.append(c)
+                else:
+                    res[c] = o
+            todo = again
+        for c in range(n):
+            if c not in res:  # non-finite at every retry: keep the halved epsilon
+                hist[c].append((used[c], float("nan")))
+                eps[c] = eps_bar[c] = used[c]
+                continue
+            S, info, _, acc = res[c]
+            rate = float(np.mean(acc))
+            hist[c].append((used[c], rate))
+            eps[c], eps_bar[c], h_bar[c] = dual_average_update(
+                eps0[c], eps_bar[c], h_bar[c], r + 1, math.log(rate) if rate > 0 else -math.inf,
+                ads[c])
+            x[c] = np.asarray(S[:, -1], chains[c][1].dtype).copy()
+    adapted = [(m, replace(s, epsilon=eps_bar[c]), x[c], seed, block)
+               for c, (m, s, _, seed, block) in enumerate(chains)]
+    return adapted, hist

@@ -343,7 +343,13 @@ def sample(model: DensityModel, sampler: ParallelMALASampler, N: int, *, seed: i
            initial_params=None, device: int = 0, handle: Optional[L.Handle] = None,
            progress: bool = False, chain_type=None, **kw) -> Chain:
     """sample(rng, model, ParallelMALASampler(...), N): ceil(N/T) DEER blocks solved
-    on the GPU, block b with tape block b of `seed` (interface.jl:557-607)."""
+    on the GPU, block b with tape block b of `seed` (interface.jl:557-607).  With an
+    AdaptiveMALASampler: its sequential adaptive chain on the device
+    (pmcmc.adapt.sample_adaptive)."""
+    if type(sampler).__name__ == "AdaptiveMALASampler":
+        from .adapt import sample_adaptive
+        return sample_adaptive(model, sampler, N, seed=seed, initial_params=initial_params,
+                               device=device, handle=handle)
     if kw.get("callback") is not None or kw.get("num_warmup", 0) or kw.get("thinning", 1) != 1 \
             or kw.get("discard_initial", 0):
         return _sample_generic(model, sampler, N, seed=seed, initial_params=initial_params,

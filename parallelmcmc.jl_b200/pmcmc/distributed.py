@@ -205,3 +205,72 @@ def local_tsplit(model, sampler, x0, nslices: int, *, seed: int = 0, block: int 
     S = np.concatenate([r.S for r in res], axis=1)
     acc = np.concatenate([r.accept for r in res])
     return S, acc, res[0].iters, res[0].converged
+
+
+# --------------------------------------------------------------------------- chains across GPUs
+def chain_cost(model, sampler) -> float:
+    """Work estimate of one chain's block: D N T for the logistic target (two
+    contraction passes of N x D by T a sweep), D^2 T for the dense Gaussian,
+    D T for the diagonal one."""
+    tg = model.target or {}
+    D, T = model.dim, int(sampler.T)
+    if tg.get("kind") == "logistic":
+        return float(D) * tg["X"].shape[0] * T
+    if tg.get("kind") == "dense_gauss":
+        return float(D) * D * T
+    return float(D) * T
+
+
+def partition_chains(costs: Sequence[float], nranks: int) -> list[list[int]]:
+    """Longest-first assignment of independent chains to ranks: chains in
+    descending cost (index breaks ties) each go to the rank with the least work
+    so far (lowest rank breaks ties).  Every rank computes the same partition
+    from the same costs, so no message is needed to agree on it.  Rank r's list
+    is in assignment order (its largest chain first)."""
+    if nranks < 1:
+        raise ArgumentError("need at least one rank")
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * nranks
+    parts: list[list[int]] = [[] for _ in range(nranks)]
+    for i in order:
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += float(costs[i])
+    return parts
+
+
+def fleet_solve_distributed(chains, *, group=None, workers: int = 8, device: Optional[int] = None,
+                            errors: str = "report", gather: bool = True, solve=None):
+    """Independent chains across ranks, one process per GPU (the MCMCThreads
+    fleet of src/interface.jl:753-775, test/test-DEER-Interface.jl:300-318,
+    spread over GPUs).  `chains` is the whole fleet, the same list on every
+    rank, as for pmcmc.fleet_solve.  Every rank solves the chains
+    partition_chains gives it with fleet_solve on its own GPU (`device`,
+    default LOCAL_RANK); the chains share nothing, so no collective runs while
+    they solve.  With gather=True the results are exchanged once at the end
+    and every rank returns the list for all chains in their order; otherwise a
+    dict {chain index: result} of this rank's chains.  `solve` replaces
+    fleet_solve (tests on CPU)."""
+    import os
+
+    import torch.distributed as dist
+
+    from . import core
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    parts = partition_chains([chain_cost(m, s) for m, s, *_ in chains], world)
+    mine = parts[rank]
+    if solve is None:
+        dev = int(os.environ.get("LOCAL_RANK", 0)) if device is None else device
+        solve = lambda cs: core.fleet_solve(cs, workers=workers, device=dev, errors=errors)
+    res = solve([chains[i] for i in mine]) if mine else []
+    local = list(zip(mine, res))
+    if not gather:
+        return dict(local)
+    every = [None] * world
+    dist.all_gather_object(every, local, group=group)
+    out = [None] * len(chains)
+    for lst in every:
+        for i, r in lst:
+            out[i] = r
+    return out

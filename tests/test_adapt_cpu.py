@@ -60,3 +60,54 @@ def test_adapt_arguments_are_checked():
         pmcmc.adapt_step_size(model, s, np.zeros(3), method="newton")
     with pytest.raises(pmcmc.ArgumentError):
         pmcmc.adapt_step_size(model, s, np.zeros(3), n_blocks=0)
+
+
+def test_oracle_adaptive_chain_has_the_reference_properties():
+    # the oracle's AdaptiveMALASampler chain (the checker of the device chains) on a
+    # standard normal, test-Adaptive-MALA.jl:117-168: the step size moves during warmup,
+    # is frozen at epsilon_bar after it, and the adapted rate is near the target
+    import oracle as O
+    D, n_w, T = 5, 2000, 2500
+    tg = O.Target.diag_gauss(np.ones(D))
+    Xi, u = O.tape(42, 0, D, T)
+    S, acc, used, (eps, eps_bar, h_bar) = O.mala_adaptive(tg, 0.5, np.zeros(D), Xi, u, n_w)
+    assert len(set(used[:n_w].tolist())) > 100
+    assert np.all(used[n_w:] == eps_bar)
+    assert 0.35 < acc[n_w:].mean() < 0.80
+    # the oracle's update and the product's host update are the same formula
+    ad = AdaptiveMALASampler(0.5)
+    np.testing.assert_allclose(O.dual_average(0.5, 0.3, 0.01, 7, -0.4),
+                               dual_average_update(0.5, 0.3, 0.01, 7, -0.4, ad), rtol=1e-14)
+
+
+def test_adapt_fleet_with_a_stand_in_solver():
+    # the fleet-level dual averaging with a stand-in for fleet_solve: the accept rate
+    # falls with epsilon (rate = exp(-eps / s_c)), a block above 4 s_c goes non-finite
+    from pmcmc import _lib as L
+    from pmcmc.adapt import adapt_fleet
+    scales = [0.01, 0.05, 0.2]
+    chains = [(pmcmc.DensityModel.diag_gaussian(np.ones(2)),
+               pmcmc.ParallelMALASampler(1.0, T=64), np.zeros(2), 7 + c, 0) for c in range(3)]
+    seen = []
+
+    def solve(batch):
+        out = []
+        for m, smp, x0, seed, block in batch:
+            s = scales[seed - 7]
+            seen.append((seed, block, smp.T))
+            if smp.epsilon > 4 * s:
+                out.append((None, {"status": L.ERR_NONFINITE}, None, None))
+                continue
+            k = int(round(smp.T * np.exp(-smp.epsilon / s)))
+            acc = np.arange(smp.T) < k
+            out.append((np.full((2, smp.T), float(seed)), {"status": 0}, None, acc))
+        return out
+
+    adapted, hist = adapt_fleet(chains, rounds=40, T_adapt=200, solve=solve)
+    for c, s in enumerate(scales):
+        eps = adapted[c][1].epsilon
+        # the target accept rate 0.574 is reached at eps = -s log(0.574) = 0.555 s
+        assert 0.3 * s < eps < 1.2 * s, (c, eps / s)
+        assert adapted[c][1].T == 64 and np.all(adapted[c][2] == 7 + c)
+        assert all(e <= 4 * s * 4 for e, _ in hist[c])
+    assert {b for _, b, _ in seen} == set(range(1, 41)) and {t for *_, t in seen} == {200}
