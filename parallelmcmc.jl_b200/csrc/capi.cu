@@ -1221,7 +1221,8 @@ int status_error(pmcmc_handle* h, int status) {
 // pmcmc_sample (block loop of interface.jl:584-599).
 int solve_core(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
                const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
-               void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
+               void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info,
+               int64_t t_off = 0) {
   int rc = validate(h, tg, p);
   if (rc) return rc;
   if (!x0 || !S_out) return fail(h, PMCMC_ERR_ARGUMENT, "x0 and the output must not be NULL");
@@ -1231,7 +1232,7 @@ int solve_core(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params*
   if (tg->kind == kLogistic) {
     if (p->jacobian == PMCMC_JAC_FULL)
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: :full is not built");
-    if (p->window > 0 && p->window < p->T)
+    if (p->window > 0 && p->window < p->T)  // solve_blocks runs such blocks in chunks
       return fail(h, PMCMC_ERR_UNSUPPORTED, "logistic target: no sliding window");
   }
   DeviceGuard guard(h->device);
@@ -1332,6 +1333,7 @@ int solve_core(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params*
   P.Dp = Dp;
   P.T = T;
   P.W = W;
+  P.t_off = static_cast<int32_t>(t_off);  // tape column of local column 0 (a chunk of the block)
   P.eps = p->epsilon;
   P.sqrt2eps = std::sqrt(2 * p->epsilon);
   P.inv4eps = 1.0 / (4 * p->epsilon);
@@ -1563,11 +1565,65 @@ int solve_mass(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params*
   return PMCMC_OK;
 }
 
+// Logistic target with a window W < T: every block is solved as consecutive
+// chunks of W columns, chunk k a DEER solve of its own from the last state of
+// chunk k - 1 on tape columns [k W, k W + W) of the block (the tape, the
+// uniforms and the probes are drawn at the block's column index).  The chain is
+// Markov, so the chunks' fixed points together are the block's: the same
+// sequential chain.  Each chunk's Newton solve sees only W columns, and the
+// number of sweeps a DEER solve needs grows with its length.  The info adds the
+// chunks' sweeps and accepts and keeps the worst metric, margin and defect.
+int solve_chunks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                 const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
+                 void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
+  int rc = validate(h, tg, p);
+  if (rc) return rc;
+  if (!x0 || !S_out) return fail(h, PMCMC_ERR_ARGUMENT, "x0 and the output must not be NULL");
+  if (N < 1) return fail(h, PMCMC_ERR_ARGUMENT, "the number of samples must be >= 1");
+  const size_t es = p->dtype == PMCMC_F64 ? 8 : 4;
+  const int64_t T = p->T, W = p->window, D = tg->D;
+  const int64_t nblocks = (N + T - 1) / T;
+  pmcmc_info agg{};
+  agg.converged = 1;
+  agg.min_margin = INFINITY;
+  const unsigned char* xprev = static_cast<const unsigned char*>(x0);
+  unsigned char* S = static_cast<unsigned char*>(S_out);
+  unsigned char* lp = static_cast<unsigned char*>(logp_out);
+  rc = PMCMC_OK;
+  for (int64_t b = 0; b < nblocks && rc == PMCMC_OK; ++b) {
+    const int64_t nkeep = std::min(T, N - b * T);
+    for (int64_t t0 = 0; t0 < nkeep && rc == PMCMC_OK; t0 += W) {
+      pmcmc_deer_params pc = *p;
+      pc.T = std::min(W, T - t0);
+      pc.window = 0;
+      const int64_t keep = std::min(pc.T, nkeep - t0), col = b * T + t0;
+      pmcmc_info ci{};
+      rc = solve_core(h, tg, &pc, xprev, seed, block0 + static_cast<uint64_t>(b), keep,
+                      S + es * col * D, lp ? lp + es * col : nullptr,
+                      accept_out ? accept_out + col : nullptr, mem, &ci, t0);
+      agg.iters += ci.iters;
+      agg.converged &= ci.converged;
+      agg.metric = std::isnan(ci.metric) ? ci.metric : std::max(agg.metric, ci.metric);
+      agg.n_accept += ci.n_accept;
+      agg.min_margin = std::min(agg.min_margin, ci.min_margin);
+      agg.max_defect = std::isnan(ci.max_defect) ? ci.max_defect
+                                                 : std::max(agg.max_defect, ci.max_defect);
+      if (ci.status && !agg.status) agg.status = ci.status;
+      agg.path |= ci.path;
+      xprev = S + es * (col + keep - 1) * D;  // the next chunk starts from this one's end
+    }
+  }
+  if (info) *info = agg;
+  return rc;
+}
+
 int solve_blocks(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
                  const void* x0, uint64_t seed, uint64_t block0, int64_t N, void* S_out,
                  void* logp_out, uint8_t* accept_out, int32_t mem, pmcmc_info* info) {
   if (tg && tg->mass_Ld)
     return solve_mass(h, tg, p, x0, seed, block0, N, S_out, logp_out, accept_out, mem, info);
+  if (tg && p && tg->kind == kLogistic && p->window > 0 && p->window < p->T)
+    return solve_chunks(h, tg, p, x0, seed, block0, N, S_out, logp_out, accept_out, mem, info);
   return solve_core(h, tg, p, x0, seed, block0, N, S_out, logp_out, accept_out, mem, info);
 }
 

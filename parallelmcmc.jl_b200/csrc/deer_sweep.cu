@@ -62,7 +62,8 @@ __device__ __forceinline__ void column_logistic(const DevParams& P, const TapeKe
       load4(hvp + 4 * j, hvy[q]);
       float xi[4];
       load4(P.xi + off + 4 * j, xi);
-      const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5), static_cast<uint32_t>(t),
+      const U4 pb = probe_bits(key, static_cast<uint32_t>(j >> 5),
+                               static_cast<uint32_t>(t + P.t_off),
                                probe, iter);
       const uint32_t wv = u4_word(pb, (j >> 3) & 3);
       const int sh = (j & 7) * 4;

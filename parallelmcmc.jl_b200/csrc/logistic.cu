@@ -76,7 +76,8 @@ __global__ void lg_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
         if (!tangent) {
           v = (from_x0 || t == 0) ? x0[d] : S[(t - 1) * Dp + d];
         } else {
-          const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t),
+          const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7),
+                                   static_cast<uint32_t>(t + P.t_off),
                                    probe, iter);
           v = ((u4_word(pb, static_cast<int>((d >> 5) & 3)) >> (d & 31)) & 1u) ? Real(1)
                                                                               : Real(-1);
@@ -181,7 +182,8 @@ __global__ void lg_mid_kernel(const DevParams* __restrict__ Pg, const DevState* 
         xi[2] = v.z;
         xi[3] = v.w;
       }
-      const U4 pb = probe_bits(key, static_cast<uint32_t>(q >> 5), static_cast<uint32_t>(t),
+      const U4 pb = probe_bits(key, static_cast<uint32_t>(q >> 5),
+                               static_cast<uint32_t>(t + P.t_off),
                                probe, iter);
       const uint32_t wv = u4_word(pb, static_cast<int>((q >> 3) & 3));
       const int sh = static_cast<int>(q & 7) * 4;

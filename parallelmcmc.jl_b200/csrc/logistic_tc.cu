@@ -535,7 +535,8 @@ __global__ void tc_prep_kernel(const DevParams* __restrict__ Pg, const DevState*
     if (d < P.D) {
       if (mode == 0) {
         v = static_cast<float>((from_x0 || t == 0) ? x0[d] : S[(t - 1) * P.Dp + d]);
-        const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7), static_cast<uint32_t>(t),
+        const U4 pb = probe_bits(key, static_cast<uint32_t>(d >> 7),
+                                 static_cast<uint32_t>(t + P.t_off),
                                  probe, iter);
         tv = ((u4_word(pb, static_cast<int>((d >> 5) & 3)) >> (d & 31)) & 1u) ? 1.f : -1.f;
       } else if (mode == 1) {
