@@ -198,14 +198,20 @@ int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q);
 
 /* pmcmc_deer_adjoint (no counterpart in the reference): gradient of an
  * objective of a solved trajectory with the accept decisions of that
- * trajectory held fixed, by one reverse scan.  S is the D x T (FP32)
- * trajectory returned by pmcmc_deer_solve for the same (p, x0, seed, block),
+ * trajectory held fixed, by a reverse scan.  S is the D x T trajectory
+ * returned by pmcmc_deer_solve for the same (p, x0, seed, block),
  * in `mem`; grad (host, 1 + D doubles) receives dL/depsilon in grad[0] and,
  * for PMCMC_OBJ_MEAN_SQ, dL/dlog s_i in grad[1 + i] for the covariance
  * eigenvalues s_i = 1 / lam_i in pmcmc_target_eigen's order (zeros for
  * PMCMC_OBJ_ESJD).  Objectives:
  *   PMCMC_OBJ_ESJD     (1/T) sum_t min(1, alpha_t) |y_t - x_{t-1}|^2
- *   PMCMC_OBJ_MEAN_SQ  (1/T) sum_t |x_t|^2 */
+ *   PMCMC_OBJ_MEAN_SQ  (1/T) sum_t |x_t|^2
+ * Gaussian targets: FP32 state, D <= 128, one reverse scan in the eigenbasis.
+ * Logistic targets: FP32 or FP64 state (S and x0 of p->dtype), computed in FP64;
+ * the reverse recurrence with the dense Jacobians I + eps H(x_t) is solved by
+ * Jacobi iterations on its diagonal (at most p->maxiter, to 1e-12 relative;
+ * PMCMC_ERR_TIMEOUT if they do not get there); grad[1 .. D] are NaN (no density
+ * parameter).  Mass-matrix targets return PMCMC_ERR_UNSUPPORTED. */
 typedef enum { PMCMC_OBJ_ESJD = 0, PMCMC_OBJ_MEAN_SQ = 1 } pmcmc_objective;
 int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* t, const pmcmc_deer_params* p,
                        const void* x0, uint64_t seed, uint64_t block, const void* S,

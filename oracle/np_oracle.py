@@ -314,3 +314,104 @@ def deer_solve_batched(model, eps, s0, Xi, u, probe, *, tol_abs=1e-6, tol_rel=1e
         if metric <= 1:
             return S, {"iters": it, "converged": True, "metric": float(metric)}
     return S, {"iters": it, "converged": False, "metric": float(metric)}
+
+
+# ---------------------------------------------------------------------------
+# Objectives of a logistic-regression trace and their adjoint (no counterpart
+# in the reference; the checks of the device adjoint).  The same recursion as
+# gauss_adjoint with the state-dependent Jacobian J_t = I + eps H(x_{t-1}) of an
+# accepted step, H the dense Hessian of bayes_logreg.jl:30-86 (prior N(0, I/tau)).
+# ---------------------------------------------------------------------------
+
+def logistic_parts(X, y, tau=1.0):
+    """(logp, grad, hess) of the logistic target, dense, FP64."""
+    X = np.asarray(X, np.float64)
+    y = np.asarray(y, np.float64)
+
+    def logp(th):
+        L = X @ th
+        return float(np.sum(y * L - _softplus(L)) - 0.5 * tau * th @ th)
+
+    def grad(th):
+        return X.T @ (y - 1.0 / (1.0 + np.exp(-(X @ th)))) - tau * th
+
+    def hess(th):
+        p = 1.0 / (1.0 + np.exp(-(X @ th)))
+        return -(X.T * (p * (1 - p))) @ X - tau * np.eye(X.shape[1])
+
+    return logp, grad, hess
+
+
+def logistic_objectives(X, y, eps, x0, Xi, u, tau=1.0):
+    """Sequential FP64 trace of the logistic target and its two objectives
+    esjd = (1/T) sum_t min(1, alpha_t) |y_t - x_{t-1}|^2 and msq = (1/T) sum_t
+    |x_t|^2.  Returns (esjd, msq, S, acc)."""
+    logp, grad, _ = logistic_parts(X, y, tau)
+    D, T = Xi.shape
+    S = np.empty((D, T))
+    acc = np.zeros(T, bool)
+    x = np.asarray(x0, np.float64)
+    esjd = 0.0
+    c = np.sqrt(2 * eps)
+    for t in range(T):
+        xi = Xi[:, t].astype(np.float64)
+        gx = grad(x)
+        yv = x + eps * gx + c * xi
+        gy = grad(yv)
+        q = x - yv - eps * gy
+        la = logp(yv) - logp(x) - q @ q / (4 * eps) + 0.5 * xi @ xi
+        acc[t] = np.log(u[t]) < la
+        esjd += min(1.0, np.exp(min(la, 0.0))) * float((yv - x) @ (yv - x))
+        x = yv if acc[t] else x
+        S[:, t] = x
+    return esjd / T, float(np.sum(S * S)) / T, S, acc
+
+
+def logistic_adjoint(X, y, eps, x0, Xi, u, S, objective, tau=1.0):
+    """d objective / d eps at the trajectory S (D, T) with its accept flags held
+    fixed: the local terms at every step, then lambda_t = c_t + J_{t+1}^T
+    lambda_{t+1} with J_{t+1} = I + eps H(x_t) (accepted) or I, solved
+    sequentially with dense Hessians."""
+    logp, grad, hess = logistic_parts(X, y, tau)
+    D, T = S.shape
+    c2 = np.sqrt(2 * eps)
+    cvec = np.zeros((D, T))
+    acc = np.zeros(T, bool)
+    dys = np.zeros((D, T))
+    Hs = []
+    direct = 0.0
+    for t in range(T):
+        xb = np.asarray(x0, float) if t == 0 else S[:, t - 1]
+        xi = Xi[:, t].astype(float)
+        gx = grad(xb)
+        yv = xb + eps * gx + c2 * xi
+        gy = grad(yv)
+        q = xb - yv - eps * gy
+        la = logp(yv) - logp(xb) - q @ q / (4 * eps) + 0.5 * xi @ xi
+        acc[t] = np.log(u[t]) < la
+        Hx, Hy = hess(xb), hess(yv)
+        Hs.append(Hx)
+        dy = gx + xi / c2
+        dys[:, t] = dy
+        if objective == "mean_sq":
+            cvec[:, t] += 2.0 * S[:, t] / T
+            continue
+        alpha = min(1.0, np.exp(min(la, 0.0)))
+        dalpha = alpha if la < 0 else 0.0
+        e = yv - xb
+        e2 = float(e @ e)
+        dq = -(dy + eps * (Hy @ dy)) - gy
+        dla = gy @ dy - q @ dq / (2 * eps) + (q @ q) / (4 * eps ** 2)
+        direct += (dalpha * dla * e2 + alpha * 2.0 * (e @ dy)) / T
+        if t >= 1:
+            Jx = np.eye(D) + eps * Hx
+            w = q + eps * (Hy @ q)
+            v = Jx @ gy - gx - (q - Jx @ w) / (2 * eps)
+            cvec[:, t - 1] += (dalpha * e2 * v + alpha * 2.0 * eps * (Hx @ e)) / T
+    lam = np.zeros((D, T))
+    lam[:, T - 1] = cvec[:, T - 1]
+    for t in range(T - 2, -1, -1):
+        nxt = lam[:, t + 1]
+        lam[:, t] = cvec[:, t] + ((nxt + eps * (Hs[t + 1] @ nxt)) if acc[t + 1] else nxt)
+    geps = direct + sum(float(lam[:, t] @ dys[:, t]) for t in range(T) if acc[t])
+    return geps

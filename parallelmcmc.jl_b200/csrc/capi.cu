@@ -715,6 +715,21 @@ int tie_kmax(int64_t T) { return static_cast<int>(std::min<int64_t>(kTieMax, T))
 // are decided in FP64 before the sweep (`refine`).  Then, on the fused path, a
 // verification pass at the returned trajectory (its passes at x_bar_t =
 // S_{t-1}: accept flags, margins, defect) and a logp pass over it.
+// The handle's cuBLAS (pedantic math, a workspace of its own so that cuBLAS
+// allocates nothing during a solve), on the handle's stream.
+int ensure_cublas(pmcmc_handle* h) {
+  if (!h->cublas) {
+    if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
+      return fail(h, PMCMC_ERR_CUDA, "cublasCreate failed");
+    cublasSetMathMode(h->cublas, CUBLAS_PEDANTIC_MATH);
+    CK(cudaMalloc(&h->cublas_ws, kCublasWsBytes));
+    if (cublasSetWorkspace(h->cublas, h->cublas_ws, kCublasWsBytes) != CUBLAS_STATUS_SUCCESS)
+      return fail(h, PMCMC_ERR_CUDA, "cublasSetWorkspace failed");
+  }
+  cublasSetStream(h->cublas, h->stream);
+  return PMCMC_OK;
+}
+
 int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k, bool coop,
                  DevParams P, const SolveLayout& L, size_t es, size_t smem_sweep,
                  int fin_grid, int init_grid, int64_t Tc, bool use_tc, bool plain) {
@@ -730,16 +745,8 @@ int run_logistic(pmcmc_handle* h, const pmcmc_target* tg, const SweepKernels& k,
   CK(cudaMemcpyAsync(h->d_params, &P, sizeof(DevParams), cudaMemcpyHostToDevice, h->stream));
   if (smem_sweep > 0)
     CK(raise_smem_limit(reinterpret_cast<const void*>(coop ? k.sweep_coop : k.sweep), smem_sweep));
-  if (!h->cublas) {
-    if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS)
-      return fail(h, PMCMC_ERR_CUDA, "cublasCreate failed");
-    cublasSetMathMode(h->cublas, CUBLAS_PEDANTIC_MATH);
-    // a workspace of its own: cuBLAS then allocates nothing during the solve
-    CK(cudaMalloc(&h->cublas_ws, kCublasWsBytes));
-    if (cublasSetWorkspace(h->cublas, h->cublas_ws, kCublasWsBytes) != CUBLAS_STATUS_SUCCESS)
-      return fail(h, PMCMC_ERR_CUDA, "cublasSetWorkspace failed");
-  }
-  cublasSetStream(h->cublas, h->stream);
+  int rc = ensure_cublas(h);
+  if (rc) return rc;
   void* init_args[] = {&h->d_params, &h->d_state};
   CK(cudaLaunchKernel(k.init, dim3(init_grid), dim3(256), init_args, 0, h->stream));
   cudaGraphConditionalHandle none = 0;
@@ -2401,6 +2408,62 @@ int pmcmc_target_eigen(pmcmc_target* t, double* lam, double* Q) {
   return PMCMC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+int scan_device(void* ctx, int64_t D, int64_t T, const double* A, const double* B,
+                const double* s0, double* S) {
+  return pmcmc_affine_scan_diag(static_cast<pmcmc_handle*>(ctx), PMCMC_F64, D, T, A, B, s0, S,
+                                PMCMC_MEM_DEVICE);
+}
+
+// The logistic adjoint (logistic_adjoint.cu): x0 and S staged on the device,
+// X .* X made on first use, the Jacobi iterations capped at p->maxiter.
+int adjoint_logistic(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
+                     const void* x0, uint64_t seed, uint64_t block, const void* S, int32_t mem,
+                     int32_t objective, double* grad) {
+  DeviceGuard guard(h->device);
+  const bool f64 = p->dtype == PMCMC_F64;
+  const size_t es = f64 ? 8 : 4;
+  const int64_t D = tg->D, T = p->T;
+  int rc = ensure_cublas(h);
+  if (rc) return rc;
+  {
+    static std::mutex square_mu;  // targets are shared across handles
+    std::lock_guard<std::mutex> lk(square_mu);
+    CK(lg_make_square(h->stream, const_cast<pmcmc_target*>(tg)->lg, true));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t bx = up(es * D), bS = up(es * T * D);
+  rc = ensure_ws(h, bx + bS + lg_adjoint_ws_bytes(tg->lg, T));
+  if (rc) return rc;
+  unsigned char* ws = h->ws;
+  const cudaMemcpyKind kin =
+      mem == PMCMC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(ws, x0, es * D, kin, h->stream));
+  CK(cudaMemcpyAsync(ws + bx, S, es * T * D, kin, h->stream));
+  double g = 0.0;
+  int iters = 0;
+  rc = lg_adjoint(h->stream, h->cublas, tg->lg, f64, ws, ws + bx, seed, block, T, p->epsilon,
+                  objective == PMCMC_OBJ_ESJD, ws + bx + bS, p->maxiter, &g, &iters, scan_device,
+                  h);
+  if (rc == 3) return fail(h, PMCMC_ERR_CUDA, "logistic adjoint: a CUDA or cuBLAS call failed");
+  if (rc == 4) return fail(h, PMCMC_ERR_NONFINITE, "logistic adjoint: non-finite lambda");
+  if (rc == 5)
+    return fail(h, PMCMC_ERR_TIMEOUT,
+                "logistic adjoint: the Jacobi iterations did not converge in %d", iters);
+  if (rc) return rc;  // a status of the scan
+  grad[0] = g;
+  for (int64_t d = 0; d < D; ++d) grad[1 + d] = NAN;  // no density-parameter gradient
+  return PMCMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params* p,
                        const void* x0, uint64_t seed, uint64_t block, const void* S, int32_t mem,
                        int32_t objective, double* grad) {
@@ -2412,9 +2475,9 @@ int pmcmc_deer_adjoint(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer
     return fail(h, PMCMC_ERR_ARGUMENT, "mem must be PMCMC_MEM_HOST or PMCMC_MEM_DEVICE");
   if (objective != PMCMC_OBJ_ESJD && objective != PMCMC_OBJ_MEAN_SQ)
     return fail(h, PMCMC_ERR_ARGUMENT, "objective must be PMCMC_OBJ_ESJD or PMCMC_OBJ_MEAN_SQ");
-  if (tg->kind == kLogistic)
-    return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for the Gaussian targets");
   if (tg->mass_Ld) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint takes no mass matrix");
+  if (tg->kind == kLogistic)
+    return adjoint_logistic(h, tg, p, x0, seed, block, S, mem, objective, grad);
   if (p->dtype != PMCMC_F32) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for FP32");
   const int64_t D = tg->D, Dp = tg->Dp, T = p->T;
   if (Dp > 128) return fail(h, PMCMC_ERR_UNSUPPORTED, "the adjoint is built for D <= 128");

@@ -79,4 +79,20 @@ int lg_tie_refine(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool 
 cudaError_t lg_verify(cudaStream_t s, bool f64, const DevParams* dP, DevState* dS, int64_t T,
                       const double* la_ref);
 
+
+// Adjoint of a trajectory objective in epsilon (logistic_adjoint.cu), FP64:
+// x0 (D) and S (T x D rows) of the state's type on the device, the tape of
+// (seed, block); esjd = 1 for the expected squared jump distance, 0 for the
+// mean of |x_t|^2; `scan` runs a diagonal affine scan of T rows of Dp doubles
+// on the device (S_t = A_t S_{t-1} + B_t from s0).  Returns 0, 3 (CUDA or
+// cuBLAS error), 4 (non-finite) or 5 (the Jacobi iterations did not reach
+// 1e-12 within max_iter); *iters gets the iterations run.
+typedef int (*ScanFn)(void* ctx, int64_t D, int64_t T, const double* A, const double* B,
+                      const double* s0, double* S);
+size_t lg_adjoint_ws_bytes(const LogisticDev& X, int64_t T);
+int lg_adjoint(cudaStream_t s, cublasHandle_t cb, const LogisticDev& X, bool f64,
+               const void* x0, const void* S, uint64_t seed, uint64_t block, int64_t T,
+               double eps, int esjd, void* ws, int max_iter, double* grad_eps, int* iters,
+               ScanFn scan, void* scan_ctx);
+
 }  // namespace pmcmc

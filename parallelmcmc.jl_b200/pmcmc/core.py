@@ -516,7 +516,8 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
     objective "mean_sq": (1/T) sum_t |x_t|^2
     Returns {"d_epsilon": float, "d_log_s": (D,) or None}; d_log_s is the
     gradient with respect to the log covariance eigenvalues s_i = 1/lam_i in
-    the order of DensityModel.eigen (mean_sq only)."""
+    the order of DensityModel.eigen (mean_sq, Gaussian targets only).  The logistic
+    target (FP32 or FP64 state) gives d_epsilon alone."""
     if objective not in L.OBJECTIVE:
         raise ArgumentError("objective must be 'esjd' or 'mean_sq'")
     h = handle or L.default_handle(device)
@@ -526,7 +527,7 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
         Sc = _torch_ready(S.T.contiguous())
         sp = Sc.data_ptr()
     else:
-        Sc = np.ascontiguousarray(np.asarray(S).T, dtype=np.float32)
+        Sc = np.ascontiguousarray(np.asarray(S).T, dtype=sampler.dtype)
         sp = Sc.ctypes.data
     if tuple(Sc.shape) != (int(sampler.T), model.dim):
         raise DimensionMismatch("S must be D x T")
@@ -535,7 +536,9 @@ def adjoint(model: DensityModel, sampler: ParallelMALASampler, s0, S, *, objecti
     rc = L.load().pmcmc_deer_adjoint(h.ptr, tgt, C.byref(p), x0p, int(seed), int(block), sp, mem,
                                      L.OBJECTIVE[objective], g.ctypes.data)
     L.check(rc, h.ptr, "deer_adjoint")
-    return {"d_epsilon": float(g[0]), "d_log_s": g[1:].copy() if objective == "mean_sq" else None}
+    gaussian = (model.target or {}).get("kind") != "logistic"
+    return {"d_epsilon": float(g[0]),
+            "d_log_s": g[1:].copy() if objective == "mean_sq" and gaussian else None}
 
 
 # --------------------------------------------------------------------------- fleet

@@ -60,3 +60,25 @@ def test_objective_trace_matches_c_oracle():
     S2, acc2, _ = O.mala_sequential(O.Target.dense_gauss(P), eps, x0, Xi, u)
     assert np.array_equal(acc, acc2.astype(bool))
     np.testing.assert_allclose(S, S2, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("objective", ["esjd", "mean_sq"])
+def test_logistic_adjoint_matches_fd(objective):
+    # the logistic restatement against central differences of the sequential trace's
+    # objective that flip no accept decision
+    import np_oracle as NO
+    rng = np.random.default_rng(12)
+    N, D, T, eps = 60, 4, 80, 0.05
+    X = rng.standard_normal((N, D)) / np.sqrt(D)
+    y = (rng.random(N) < 1 / (1 + np.exp(-X @ rng.standard_normal(D)))).astype(float)
+    Xi, u = O.tape(3, 0, D, T)
+    x0 = rng.standard_normal(D) * 0.3
+    e0, m0, S, acc = NO.logistic_objectives(X, y, eps, x0, Xi, u)
+    assert 0 < (~acc).sum() < T
+    g = NO.logistic_adjoint(X, y, eps, x0, Xi, u, S, objective)
+    h = 1e-6 * eps
+    ep, mp, _, ap = NO.logistic_objectives(X, y, eps + h, x0, Xi, u)
+    em, mm, _, am = NO.logistic_objectives(X, y, eps - h, x0, Xi, u)
+    assert np.array_equal(ap, acc) and np.array_equal(am, acc)
+    fd = ((ep - em) if objective == "esjd" else (mp - mm)) / (2 * h)
+    assert abs(g - fd) <= 1e-5 * abs(fd) + 1e-9
