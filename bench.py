@@ -30,6 +30,7 @@ Secondary measurements (1 GPU):
     python bench.py --workload corr_gauss_d64_full   # D=64, T=8192, :full
     python bench.py --workload logistic_fleet        # 32 uneven logistic chains (N, T / 4)
     python bench.py --workload logistic_fleet_full   # all 512 chains at full N and T
+    python bench.py --workload logistic_adjoint      # the logistic adjoint at a solved block
     python bench.py --workload logistic_n10k_d256 --dim 512   # the wide tensor-core pass
 --small shrinks T (logistic 4096, correlated Gaussian 1024) for profiler captures.
 """
@@ -743,6 +744,43 @@ def run_fleet(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    """The logistic adjoint at the headline workload: one block solved on the
+    tensor cores, then d ESJD / d epsilon and d mean|x|^2 / d epsilon at the
+    returned trajectory (FP64 HVP GEMMs and Jacobi iterations), host wall clock
+    with device synchronisation."""
+    import numpy as np
+    import torch
+
+    import pmcmc
+
+    T = 4096 if args.small else 65536
+    model, sampler, x0, meta = headline(T=T)
+    h = pmcmc.Handle(0)
+    dev = torch.device("cuda", 0)
+    S, info = pmcmc.solve(model, sampler, x0, seed=meta["seed"] + 1000, block=1000, handle=h)
+    if not info["converged"]:
+        raise RuntimeError("the block did not converge")
+    out = {}
+    with ClockSampler(0) as clk:
+        for obj in ("esjd", "mean_sq"):
+            times = []
+            for _ in range(2):
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                g = pmcmc.adjoint(model, sampler, x0, S, objective=obj,
+                                  seed=meta["seed"] + 1000, block=1000, handle=h)
+                torch.cuda.synchronize(dev)
+                times.append(time.perf_counter() - t0)
+            out[obj] = {"d_epsilon": g["d_epsilon"], "ms": 1e3 * min(times)}
+    line = {"metric": "logistic adjoint d objective / d epsilon at a solved block",
+            "secondary": True, "value": out["esjd"]["ms"], "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64 (adjoint), f32 (state)",
+            "config": {"workload": workload_name(T), "newton_iters": info["iters"]},
+            "objectives": out, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_fleet_ranks(args, chains, workload):
     """The fleet on N GPUs, one process each: every rank solves the chains the
     cost-balanced partition gives it (pmcmc.distributed.fleet_solve_distributed,
@@ -918,7 +956,7 @@ def main():
                     help="skip the secondary diagonal-Gaussian measurements")
     ap.add_argument("--workload", default="logistic_n10k_d256",
                     choices=["logistic_n10k_d256", "aniso_diag_d100", "corr_gauss_d64_full",
-                             "logistic_fleet", "logistic_fleet_full"])
+                             "logistic_fleet", "logistic_fleet_full", "logistic_adjoint"])
     ap.add_argument("--dim", type=int, default=256,
                     help="logistic workload: dimension D (256 < D <= 512 runs the wide "
                          "tensor-core pass); D != 256 or --small is a secondary line")
@@ -933,6 +971,8 @@ def main():
         run_fleet(args)
     elif args.workload == "logistic_fleet_full":
         run_fleet_full(args)
+    elif args.workload == "logistic_adjoint":
+        run_adjoint(args)
     elif args.workload == "aniso_diag_d100":
         run_gauss(args)
     elif args.workload == "corr_gauss_d64_full" or args.small or args.dim != 256:

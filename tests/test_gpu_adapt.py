@@ -50,3 +50,22 @@ def test_esjd_gradient_raises_a_small_step():
     _, e0 = _accept_and_esjd(model, 0.005, x0, h)
     _, e1 = _accept_and_esjd(model, out["epsilon"], x0, h)
     assert e1 > 3 * e0, (out["epsilon"], e0, e1)
+
+
+def test_esjd_gradient_on_the_logistic_target():
+    # ESJD ascent with the logistic adjoint: a small step grows and the jump distance
+    # with it (the per-chain adaptation config 5 describes)
+    rng = np.random.default_rng(7)
+    N, D = 800, 16
+    X = rng.standard_normal((N, D)) / np.sqrt(D)
+    y = (rng.random(N) < 1 / (1 + np.exp(-X @ rng.standard_normal(D)))).astype(float)
+    model = pmcmc.DensityModel.logistic(X, y)
+    h = pmcmc.Handle(0)
+    x0 = np.zeros(D, np.float32)
+    s = pmcmc.ParallelMALASampler(0.001, T=256, dtype=np.float32, tol_abs=1e-7, tol_rel=1e-6,
+                                  maxiter=300)
+    out = pmcmc.adapt_step_size(model, s, x0, n_blocks=8, method="esjd_gradient", seed=2,
+                                handle=h)
+    assert out["history"][0]["d_esjd_d_epsilon"] > 0
+    assert out["epsilon"] > 0.004
+    assert out["history"][-1]["esjd"] > 3 * out["history"][0]["esjd"]
