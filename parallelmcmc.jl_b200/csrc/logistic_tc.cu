@@ -435,10 +435,16 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       const bool valid = n < N;
       const float yn = y_next;
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
+      if (g_owner && nb > 0) {
+        // the previous block's G partials are final once its GEMM2 has committed,
+        // and the next GEMM2 restarts G only after this block's R (bar_r): they
+        // are added while this block's X arrives and its GEMM1 runs
+        if (!(ok = mbar_wait(bar_g + (nh - 1), (nb - 1) & 1, err))) break;
+        tc_fence_after();
+        add_g();
+      }
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
-      // GEMM2 of the previous block ran before this block's GEMM1 completed
-      if (g_owner && nb > 0) add_g();
       float v[BH], vl[BH], w[BH];
       tmem_ld8x3(tL + lane_off + BH * part, tL + lane_off + 2 * BT + BH * part,
                  tL + lane_off + BT + BH * part, v, vl, w);
@@ -827,10 +833,15 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
       const bool valid = n < N;
       const float yn = y_next;
       if (n + BN < N) y_next = __ldg(ylab + n + BN);
+      if (has_g && nb > 0) {
+        // the previous block's G partials, final at its GEMM2's commit and kept
+        // until this block's R arrives: added while this block's GEMM1 runs
+        if (!(ok = mbar_wait(bar_g, (nb - 1) & 1, err))) break;
+        tc_fence_after();
+        add_g();
+      }
       if (!(ok = mbar_wait(bar_l, nb & 1, err))) break;
       tc_fence_after();
-      // GEMM2 of the previous block ran before this block's GEMM1 completed
-      if (has_g && nb > 0) add_g();
       float v[BH], vl[BH], w[BH];
       tmem_ld4x3(tL + lane_off + BH * part, tL + lane_off + 2 * BTW + BH * part,
                  tL + lane_off + BTW + BH * part, v, vl, w);
