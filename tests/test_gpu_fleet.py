@@ -69,3 +69,31 @@ def test_fleet_chains_match_the_fp64_sequential_chains():
         assert err <= 1e-5, (seed, model.dim, err)
         checked += 1
     assert checked >= 4
+
+
+def test_partitioned_fleet_on_one_rank_is_the_fleet():
+    # fleet_solve_distributed on a world of one (gloo), the device fleet underneath: the
+    # same results as fleet_solve, in chain order
+    import os
+    import socket
+
+    import torch.distributed as dist
+    from pmcmc import configs
+    from pmcmc import distributed as Dd
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        chains = configs.logistic_fleet(n_chains=6, scale=0.05)
+        h = pmcmc.Handle(0)
+        got = Dd.fleet_solve_distributed(chains, device=0)
+        ref = pmcmc.fleet_solve(chains, workers=8, handle=h, errors="report")
+        assert len(got) == len(ref)
+        for a, b in zip(got, ref):
+            assert a[1]["status"] == b[1]["status"]
+            np.testing.assert_array_equal(a[0], b[0])
+            np.testing.assert_array_equal(a[3], b[3])
+    finally:
+        dist.destroy_process_group()
