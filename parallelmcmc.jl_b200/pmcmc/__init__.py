@@ -9,7 +9,7 @@ from ._lib import (ArgumentError, DeviceError, DimensionMismatch, Handle, Unsupp
                    default_handle, load)
 from .adapt import (AdaptiveMALASampler, adapt_step_size, adaptive_chains, dual_average_update,
                     sample_adaptive)
-from .core import (Chain, Cholesky, DensityModel, ParallelMALASampler, ParallelMALAState,
+from .core import (Chain, ChainSet, Cholesky, DensityModel, MCMCThreads, ParallelMALASampler, ParallelMALAState,
                    ParallelMALATransition, adjoint, autotune, fleet_solve, mala_chains, sample,
                    solve,
                    cholesky, solve_affine_scan_diag, step, tape)
@@ -24,5 +24,6 @@ __all__ = [
     "ParallelMALAState", "ParallelMALATransition", "adjoint", "fleet_solve", "sample", "solve",
     "step", "tape", "mala_chains", "autotune", "AdaptiveMALASampler", "adapt_step_size", "dual_average_update",
     "adaptive_chains", "sample_adaptive",
-    "solve_affine_scan_diag", "DEER", "DEERScan", "Cholesky", "cholesky",
+    "solve_affine_scan_diag", "DEER", "DEERScan", "Cholesky", "cholesky", "MCMCThreads",
+    "ChainSet",
 ]

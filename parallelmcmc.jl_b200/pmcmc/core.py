@@ -339,13 +339,87 @@ def _initial_params(model, sampler, initial_params, seed):
     return np.random.default_rng(seed).standard_normal(model.dim).astype(sampler.dtype)
 
 
-def sample(model: DensityModel, sampler: ParallelMALASampler, N: int, *, seed: int = 0,
+class MCMCThreads:
+    """AbstractMCMC.MCMCThreads(): several chains side by side,
+    sample(model, sampler, MCMCThreads(), N, nchains)."""
+
+
+@dataclass
+class ChainSet:
+    """The chains of sample(model, sampler, MCMCThreads(), N, nchains)."""
+    chains: list
+
+    @property
+    def nchains(self) -> int:
+        return len(self.chains)
+
+    @property
+    def niters(self) -> int:
+        return len(self.chains[0]) if self.chains else 0
+
+    @property
+    def values(self):  # (nchains, N, D)
+        return np.stack([c.values for c in self.chains])
+
+
+def chain_seed(seed: int, c: int) -> int:
+    """Seed of chain c of a multi-chain sample() with master seed `seed`."""
+    return (int(seed) * 1000003 + 7919 * int(c) + 1) % (1 << 63)
+
+
+def _sample_threads(model, sampler, N, nchains, *, seed=0, initial_params=None, device=0,
+                    handle=None, workers=8):
+    """MCMCThreads (src/interface.jl:557-607 per chain, test/test-DEER-Interface.jl:300-318):
+    chain c has seed chain_seed(seed, c) and runs exactly the blocks sample() runs for
+    that seed; every round solves the next block of all chains together on the device
+    fleet (pmcmc_fleet_solve), each chain continuing from its last state."""
+    if N < 1 or nchains < 1:
+        raise ArgumentError("N and nchains must be >= 1")
+    h = handle or L.default_handle(device)
+    seeds = [chain_seed(seed, c) for c in range(nchains)]
+    if initial_params is None:
+        x = [np.asarray(_initial_params(model, sampler, None, sd), sampler.dtype).ravel()
+             for sd in seeds]
+    else:
+        ip = list(initial_params)
+        if len(ip) != nchains:
+            raise DimensionMismatch("one initial state per chain")
+        x = [np.asarray(v, sampler.dtype).ravel() for v in ip]
+    T = int(sampler.T)
+    vals = [np.empty((N, model.dim), sampler.dtype) for _ in range(nchains)]
+    logp = [np.empty(N, sampler.dtype) for _ in range(nchains)]
+    acc = [np.empty(N, bool) for _ in range(nchains)]
+    info = [{"iters": 0, "converged": True, "n_accept": 0} for _ in range(nchains)]
+    for b in range((N + T - 1) // T):
+        keep = min(T, N - b * T)
+        res = fleet_solve([(model, sampler, x[c], seeds[c], b) for c in range(nchains)],
+                          workers=workers, handle=h, errors="raise")
+        for c, (S, inf, lp, ac) in enumerate(res):
+            vals[c][b * T:b * T + keep] = S[:, :keep].T
+            logp[c][b * T:b * T + keep] = lp[:keep]
+            acc[c][b * T:b * T + keep] = ac[:keep]
+            info[c]["iters"] += inf["iters"]
+            info[c]["converged"] &= bool(inf["converged"])
+            info[c]["n_accept"] += int(np.sum(ac[:keep]))
+            x[c] = np.ascontiguousarray(S[:, keep - 1])
+    return ChainSet([Chain(vals[c], logp[c], acc[c], dict(info[c], seed=seeds[c]),
+                           model.param_names) for c in range(nchains)])
+
+
+def sample(model: DensityModel, sampler: ParallelMALASampler, N, *rest, seed: int = 0,
            initial_params=None, device: int = 0, handle: Optional[L.Handle] = None,
            progress: bool = False, chain_type=None, **kw) -> Chain:
     """sample(rng, model, ParallelMALASampler(...), N): ceil(N/T) DEER blocks solved
     on the GPU, block b with tape block b of `seed` (interface.jl:557-607).  With an
     AdaptiveMALASampler: its sequential adaptive chain on the device
     (pmcmc.adapt.sample_adaptive)."""
+    if isinstance(N, MCMCThreads):  # sample(model, sampler, MCMCThreads(), N, nchains)
+        if len(rest) != 2:
+            raise ArgumentError("sample(model, sampler, MCMCThreads(), N, nchains)")
+        return _sample_threads(model, sampler, int(rest[0]), int(rest[1]), seed=seed,
+                               initial_params=initial_params, device=device, handle=handle)
+    if rest:
+        raise ArgumentError("unexpected positional arguments")
     if type(sampler).__name__ == "AdaptiveMALASampler":
         from .adapt import sample_adaptive
         return sample_adaptive(model, sampler, N, seed=seed, initial_params=initial_params,

@@ -105,3 +105,16 @@ def test_no_silent_cpu_fallback_without_gpu():
     m = pmcmc.DensityModel.diag_gaussian(np.ones(2))
     with pytest.raises(pmcmc.DeviceError):
         pmcmc.sample(m, pmcmc.ParallelMALASampler(0.1), 10)
+
+
+def test_mcmcthreads_arguments():
+    import numpy as np
+    from pmcmc import ArgumentError, DensityModel, MCMCThreads, ParallelMALASampler, sample
+    m = DensityModel.diag_gaussian(np.ones(2))
+    s = ParallelMALASampler(0.1, T=8)
+    with pytest.raises(ArgumentError):
+        sample(m, s, MCMCThreads(), 10)
+    with pytest.raises(ArgumentError):
+        sample(m, s, MCMCThreads(), 0, 2)
+    with pytest.raises(ArgumentError):
+        sample(m, s, 10, 3)

@@ -583,3 +583,19 @@ def test_logistic_unsupported_modes(h):
         pmcmc.solve(model, pmcmc.ParallelMALASampler(0.01, T=16, jacobian="full",
                                                      dtype=np.float32), np.zeros(4, np.float32),
                     handle=h)
+
+
+def test_mcmcthreads_chains_are_the_single_chain_samples(h):
+    # sample(model, sampler, MCMCThreads(), N, nchains) (test-DEER-Interface.jl:300-318):
+    # chain c is sample() with its own seed, every block of all chains solved together
+    model = pmcmc.DensityModel.diag_gaussian(np.ones(2))
+    sampler = pmcmc.ParallelMALASampler(0.05, T=8)
+    cs = pmcmc.sample(model, sampler, pmcmc.MCMCThreads(), 40, 2, seed=42, handle=h)
+    assert cs.nchains == 2 and cs.niters == 40 and cs.values.shape == (2, 40, 2)
+    model3, sampler3, _, _ = configs.quickstart_2d()
+    cs3 = pmcmc.sample(model3, sampler3, pmcmc.MCMCThreads(), 150, 3, seed=7, handle=h)
+    for c in range(3):
+        one = pmcmc.sample(model3, sampler3, 150, seed=pmcmc.core.chain_seed(7, c), handle=h)
+        np.testing.assert_array_equal(cs3.chains[c].accepted, one.accepted)
+        np.testing.assert_allclose(cs3.chains[c].values, one.values, rtol=1e-12, atol=1e-12)
+        assert cs3.chains[c].info["converged"]
