@@ -154,3 +154,31 @@ def test_mass_unsupported_paths(h):
     with pytest.raises(pmcmc.DimensionMismatch):
         pmcmc.solve(pmcmc.DensityModel.diag_gaussian(np.ones(5)), s, np.zeros(5, np.float32),
                     handle=h)
+
+
+def test_mass_with_full_jacobian_and_in_the_fleet(h):
+    # the whitened target is a dense Gaussian, so :full (eigenbasis scan) and the fleet
+    # take it as they take any dense target
+    P, mu, M, x0 = _dense_case(16, 8)
+    model = pmcmc.DensityModel.dense_gaussian(P, mu)
+    T, eps = 512, 0.25
+    Lf = np.linalg.cholesky(M)
+    tg = O.Target.dense_gauss(P, mu)
+    full = pmcmc.ParallelMALASampler(eps, T=T, jacobian="full", dtype=np.float32, tol_abs=1e-8,
+                                     tol_rel=2e-7, maxiter=400, cholM=pmcmc.cholesky(M))
+    S, info, _, acc = pmcmc.solve(model, full, x0.astype(np.float32), seed=13, handle=h,
+                                  return_logp=True)
+    Xi, u = O.tape(13, 0, 16, T)
+    S_seq, acc_seq, _ = O.mala_sequential_mass(tg, eps, Lf, x0.astype(np.float32), Xi, u)
+    assert info["converged"] and info["path"] & 16
+    assert np.array_equal(acc, acc_seq)
+    assert trace_err(S, S_seq) <= 1e-5
+    diag = dataclasses.replace(full, jacobian="diag", dtype=np.float64, tol_abs=1e-12,
+                               tol_rel=1e-10)
+    chains = [(model, diag, x0 + 0.1 * k, 20 + k, 0) for k in range(4)]
+    res = pmcmc.fleet_solve(chains, workers=4, handle=h)
+    for k, (Sk, ik, _, ak) in enumerate(res):
+        Xi, u = O.tape(20 + k, 0, 16, T)
+        S_ref, acc_ref, _ = O.mala_sequential_mass(tg, eps, Lf, x0 + 0.1 * k, Xi, u)
+        assert ik["converged"] and np.array_equal(ak, acc_ref)
+        assert trace_err(Sk, S_ref) <= 1e-8
