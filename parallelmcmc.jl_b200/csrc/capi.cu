@@ -1547,11 +1547,17 @@ int solve_mass(pmcmc_handle* h, const pmcmc_target* tg, const pmcmc_deer_params*
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
   const size_t bx = up(es * D), bS = host ? up(es * N * D) : 0,
                blp = host && logp_out ? up(es * N) : 0, bac = host && accept_out ? up(N) : 0;
+  // stream-ordered scratch: freeing it does not wait for the device (fleet workers
+  // on other streams keep running)
   struct Scratch {
     void* buf = nullptr;
-    ~Scratch() { cudaFree(buf); }
+    cudaStream_t s = nullptr;
+    ~Scratch() {
+      if (buf) cudaFreeAsync(buf, s);
+    }
   } sc;
-  CK(cudaMalloc(&sc.buf, 2 * bx + bS + blp + bac));
+  sc.s = h->stream;
+  CK(cudaMallocAsync(&sc.buf, 2 * bx + bS + blp + bac, h->stream));
   unsigned char* b = static_cast<unsigned char*>(sc.buf);
   CK(cudaMemcpyAsync(b, x0, es * D, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                      h->stream));
