@@ -869,7 +869,8 @@ def run_fleet_full(args):
             # blocks of the whole batch, the chain moving on from block to block
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            chains, hist = adapt_fleet(chains0, rounds=rounds, T_adapt=t_adapt, handle=h)
+            chains, hist = adapt_fleet(chains0, rounds=rounds, T_adapt=t_adapt, handle=h,
+                                       method=args.adapt)
             torch.cuda.synchronize()
             adapt_s += time.perf_counter() - t0
             t0 = time.perf_counter()
@@ -923,8 +924,8 @@ def run_fleet_full(args):
             "value_with_adaptation": samples / (total_s + adapt_s),
             "config": {"workload": f"logistic_fleet_{n_total}chains_full", "chains": n_total,
                        "batch": batch, "workers": 8,
-                       "adaptation": f"dual averaging, {rounds} rounds of {t_adapt}-step blocks "
-                                     f"per chain from eps = 0.5 / sqrt(D)",
+                       "adaptation": f"{args.adapt.replace('_', ' ')}, {rounds} rounds of "
+                                     f"{t_adapt}-step blocks per chain from eps = 0.5 / sqrt(D)",
                        "T_total_all": sum(c["T"] for c in per), "T_total_converged": samples,
                        "converged": len(ok),
                        "not_converged": sum(1 for c in per if not c["converged"] and
@@ -960,6 +961,9 @@ def main():
     ap.add_argument("--dim", type=int, default=256,
                     help="logistic workload: dimension D (256 < D <= 512 runs the wide "
                          "tensor-core pass); D != 256 or --small is a secondary line")
+    ap.add_argument("--adapt", default="dual_averaging",
+                    choices=["dual_averaging", "esjd_gradient"],
+                    help="logistic_fleet_full: per-chain step-size adaptation before the solves")
     ap.add_argument("--small", action="store_true",
                     help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()

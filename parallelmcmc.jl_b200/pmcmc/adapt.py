@@ -245,10 +245,17 @@ def adapt_step_size(model: DensityModel, sampler: ParallelMALASampler, x0, *,
 
 def adapt_fleet(chains, *, rounds: int = 8, T_adapt: int = 256, target_accept: float = 0.574,
                 max_step_ratio: float = 4.0, retries: int = 6, workers: int = 8,
-                handle: Optional[L.Handle] = None, device: int = 0, solve=None):
-    """Per-chain dual averaging of epsilon for a fleet (`chains` as for
+                handle: Optional[L.Handle] = None, device: int = 0, solve=None,
+                method: str = "dual_averaging", step0: float = 0.5, grad=None):
+    """Per-chain step-size adaptation for a fleet (`chains` as for
     pmcmc.fleet_solve), every round one short block of every chain solved
     together on the fleet.
+
+    method "esjd_gradient": after round r, log epsilon += step0 / sqrt(r + 1) *
+    sign(d ESJD / d epsilon) with the gradient from the adjoint at the block
+    (pmcmc.adjoint; `grad(chain, x_start, S)` replaces it in tests), as
+    adapt_step_size does for one chain; the result is the last epsilon.
+    method "dual_averaging", the default, is described below.
 
     Round r: chain c solves tape block `block_c + 1 + r` of its seed, T_adapt
     steps at its current epsilon from its current state; the block's accept
@@ -267,9 +274,16 @@ def adapt_fleet(chains, *, rounds: int = 8, T_adapt: int = 256, target_accept: f
 
     if rounds < 1 or T_adapt < 1:
         raise ArgumentError("rounds and T_adapt must be >= 1")
-    if solve is None:
+    if method not in ("dual_averaging", "esjd_gradient"):
+        raise ArgumentError("method must be 'dual_averaging' or 'esjd_gradient'")
+    h = None
+    if solve is None or (method == "esjd_gradient" and grad is None):
         h = handle or L.default_handle(device)
+    if solve is None:
         solve = lambda cs: fleet_solve(cs, workers=workers, handle=h, errors="report")
+    if grad is None:
+        grad = lambda ch, xs, S: adjoint(ch[0], ch[1], xs, S, objective="esjd", seed=ch[3],
+                                         block=ch[4], handle=h)["d_epsilon"]
     n = len(chains)
     eps0 = [float(s.epsilon) for _, s, *_ in chains]
     ads = [AdaptiveMALASampler(e, target_accept=target_accept) for e in eps0]
@@ -303,9 +317,17 @@ def adapt_fleet(chains, *, rounds: int = 8, T_adapt: int = 256, target_accept: f
             S, info, _, acc = res[c]
             rate = float(np.mean(acc))
             hist[c].append((used[c], rate))
-            eps[c], eps_bar[c], h_bar[c] = dual_average_update(
-                eps0[c], eps_bar[c], h_bar[c], r + 1, math.log(rate) if rate > 0 else -math.inf,
-                ads[c])
+            if method == "dual_averaging":
+                eps[c], eps_bar[c], h_bar[c] = dual_average_update(
+                    eps0[c], eps_bar[c], h_bar[c], r + 1,
+                    math.log(rate) if rate > 0 else -math.inf, ads[c])
+            else:
+                ch = (chains[c][0], replace(chains[c][1], epsilon=used[c], T=int(T_adapt)),
+                      None, chains[c][3], chains[c][4] + 1 + r)
+                d = grad(ch, x[c], S)
+                step = step0 / math.sqrt(r + 1.0) * (math.copysign(1.0, d)
+                                                     if d != 0.0 and math.isfinite(d) else 0.0)
+                eps[c] = eps_bar[c] = used[c] * math.exp(step)
             x[c] = np.asarray(S[:, -1], chains[c][1].dtype).copy()
     adapted = [(m, replace(s, epsilon=eps_bar[c]), x[c], seed, block)
                for c, (m, s, _, seed, block) in enumerate(chains)]

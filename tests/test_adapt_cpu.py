@@ -111,3 +111,26 @@ def test_adapt_fleet_with_a_stand_in_solver():
         assert adapted[c][1].T == 64 and np.all(adapted[c][2] == 7 + c)
         assert all(e <= 4 * s * 4 for e, _ in hist[c])
     assert {b for _, b, _ in seen} == set(range(1, 41)) and {t for *_, t in seen} == {200}
+
+
+def test_adapt_fleet_esjd_gradient_with_stand_ins():
+    # the gradient method of adapt_fleet: sign steps on log epsilon toward the epsilon
+    # where a stand-in ESJD gradient changes sign (eps* = 0.01 and 0.2)
+    from pmcmc.adapt import adapt_fleet
+    targets = [0.01, 0.2]
+    chains = [(pmcmc.DensityModel.diag_gaussian(np.ones(2)),
+               pmcmc.ParallelMALASampler(0.05, T=64), np.zeros(2), 30 + c, 0) for c in range(2)]
+
+    def solve(batch):
+        return [(np.zeros((2, smp.T)), {"status": 0}, None, np.ones(smp.T, bool))
+                for _, smp, *_ in batch]
+
+    def grad(ch, xs, S):
+        return targets[ch[3] - 30] - ch[1].epsilon
+
+    adapted, hist = adapt_fleet(chains, rounds=60, T_adapt=32, method="esjd_gradient",
+                                solve=solve, grad=grad)
+    for c, t in enumerate(targets):
+        assert 0.8 * t < adapted[c][1].epsilon < 1.25 * t, (c, adapted[c][1].epsilon)
+    with pytest.raises(pmcmc.ArgumentError):
+        adapt_fleet(chains, method="newton", solve=solve)
