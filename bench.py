@@ -870,7 +870,7 @@ def run_fleet_full(args):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             chains, hist = adapt_fleet(chains0, rounds=rounds, T_adapt=t_adapt, handle=h,
-                                       method=args.adapt)
+                                       method=args.adapt, target_accept=args.target_accept)
             torch.cuda.synchronize()
             adapt_s += time.perf_counter() - t0
             t0 = time.perf_counter()
@@ -925,7 +925,9 @@ def run_fleet_full(args):
             "config": {"workload": f"logistic_fleet_{n_total}chains_full", "chains": n_total,
                        "batch": batch, "workers": 8,
                        "adaptation": f"{args.adapt.replace('_', ' ')}, {rounds} rounds of "
-                                     f"{t_adapt}-step blocks per chain from eps = 0.5 / sqrt(D)",
+                                     f"{t_adapt}-step blocks per chain from eps = 0.5 / sqrt(D)"
+                                     + (f", target accept {args.target_accept}"
+                                        if args.adapt == "dual_averaging" else ""),
                        "T_total_all": sum(c["T"] for c in per), "T_total_converged": samples,
                        "converged": len(ok),
                        "not_converged": sum(1 for c in per if not c["converged"] and
@@ -964,6 +966,8 @@ def main():
     ap.add_argument("--adapt", default="dual_averaging",
                     choices=["dual_averaging", "esjd_gradient"],
                     help="logistic_fleet_full: per-chain step-size adaptation before the solves")
+    ap.add_argument("--target-accept", type=float, default=0.574,
+                    help="logistic_fleet_full with dual averaging: the accept rate it targets")
     ap.add_argument("--small", action="store_true",
                     help="secondary workloads: shorter T for profiler captures")
     args = ap.parse_args()
