@@ -8,11 +8,14 @@ contiguous slices [t0, t0 + W) that evaluate and scan locally and exchange
 only D-vectors:
 
     per sweep, on every slice r
-      1. xbar0  = last column of slice r-1's iterate (x0 for slice 0)   allgather
+      1. xbar0  = last column of slice r-1's iterate (x0 for slice 0)
       2. local  = A, B on the slice; map (prod_t A_t, b) of the slice
       3. carry  = maps of slices 0..r-1 applied to x0, in order         allgather
-      4. finish = slice rescanned from carry, damped; max|dS|, max|S|   allreduce max
-      converged when max|dS| / (tol_abs + tol_rel max|S|) <= 1 (DEER.jl:567-578)
+      4. finish = slice rescanned from carry, damped; its last column,
+                  max|dS|, max|S|                                        allgather
+      converged when max|dS| / (tol_abs + tol_rel max|S|) <= 1 (DEER.jl:567-578);
+      the last columns gathered in 4 are the next sweep's left boundaries (1),
+      so a sweep makes two exchanges
 
 The iterates are those of the single-device solve in exact arithmetic.  The
 device work of a slice runs in libpmcmc_deer.so (pmcmc_slice_*); this module is
@@ -167,26 +170,32 @@ def tsplit_solve(slices: Sequence, x0, sampler, *, seed: int = 0, block: int = 0
     bounds = [slice_bounds(int(sampler.T), ex.world, r) for r in ranks]
     for b, (t0, W) in zip(slices, bounds):
         b.begin(x0, seed, block, t0, W)
-    last = [x0.copy() for _ in slices]  # the iterate starts as x0 broadcast
+    # the iterate starts as x0 broadcast, so every slice's last column is x0: no
+    # exchange before the first sweep
+    D = x0.size
+    lasts = [x0.copy() for _ in range(ex.world)]
     converged, metric, it = False, float("inf"), 0
     for it in range(1, int(sampler.maxiter) + 1):
-        lasts = ex.allgather(last)
         aggs_local = [b.local(x0 if r == 0 else lasts[r - 1]) for b, r in zip(slices, ranks)]
         aggs = ex.allgather([a.reshape(-1) for a in aggs_local])
-        dmax, smax = 0.0, 0.0
-        for i, (b, r) in enumerate(zip(slices, ranks)):
+        packed = []
+        for b, r in zip(slices, ranks):
             carry = x0.copy()
             for q in range(r):
                 a = aggs[q].reshape(2, -1)
                 carry = a[0] * carry + a[1]
-            dm, sm, last[i] = b.finish(carry)
-            dmax, smax = max(dmax, dm), max(smax, sm)
-        dmax, smax = ex.allreduce_max(np.array([dmax, smax]))
+            dm, sm, last = b.finish(carry)
+            packed.append(np.concatenate([np.asarray(last, np.float64).ravel(), [dm, sm]]))
+        # one exchange: every slice's last column (the next sweep's left boundaries)
+        # together with its maxima, whose max over the slices is the convergence test
+        everyone = ex.allgather(packed)
+        lasts = [v[:D] for v in everyone]
+        dmax = max(float(v[D]) for v in everyone)
+        smax = max(float(v[D + 1]) for v in everyone)
         metric = float(dmax / (sampler.tol_abs + sampler.tol_rel * smax))
         if metric <= 1.0:
             converged = True
             break
-    lasts = ex.allgather(last)
     out = []
     for b, r, (t0, W) in zip(slices, ranks, bounds):
         S, lp, acc, info = b.result(x0 if r == 0 else lasts[r - 1])
