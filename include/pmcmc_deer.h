@@ -61,14 +61,14 @@ typedef enum { PMCMC_MEM_HOST = 0, PMCMC_MEM_DEVICE = 1 } pmcmc_mem;
  * PMCMC_EXEC_PLAIN: the reference's structure on the GPU -- separate
  *   broadcast-style kernels, Hillis-Steele doubling scan, host-synchronised
  *   convergence check every iteration, FP32 SIMT only (the "plain GPU DEER"
- *   baseline of the north-star metric). */
+ *   that the batched, mixed-precision path is measured against). */
 typedef enum { PMCMC_EXEC_FUSED = 0, PMCMC_EXEC_PLAIN = 1 } pmcmc_exec;
 
 typedef struct pmcmc_handle pmcmc_handle;
 typedef struct pmcmc_target pmcmc_target;
 
-/* ParallelMALASampler fields (src/interface.jl:248-290) plus the north-star
- * additions (:full, window) and execution controls. */
+/* ParallelMALASampler fields (src/interface.jl:248-290) plus the modes this
+ * library adds (:full, window) and execution controls. */
 typedef struct {
   double epsilon;   /* step size, > 0 */
   int64_t T;        /* trajectory length per block (reference default 64) */
