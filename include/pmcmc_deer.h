@@ -56,8 +56,11 @@ typedef enum { PMCMC_F32 = 0, PMCMC_F64 = 1 } pmcmc_dtype;
 typedef enum { PMCMC_MEM_HOST = 0, PMCMC_MEM_DEVICE = 1 } pmcmc_mem;
 
 /* Execution strategy of a solve.
- * PMCMC_EXEC_FUSED: one fused kernel per Newton sweep, the Newton loop in a
- *   CUDA graph with a device-side convergence test (the product path).
+ * PMCMC_EXEC_FUSED: the product path.  Gaussian targets: a whole solve in one
+ *   persistent launch, or one fused kernel per Newton sweep with the loop in a
+ *   CUDA graph and a device-side convergence test.  Logistic targets: the
+ *   tensor-core contraction passes and one fused finish-and-scan kernel per
+ *   sweep, the state read by the host after each sweep.
  * PMCMC_EXEC_PLAIN: the reference's structure on the GPU -- separate
  *   broadcast-style kernels, Hillis-Steele doubling scan, host-synchronised
  *   convergence check every iteration, FP32 SIMT only (the "plain GPU DEER"
